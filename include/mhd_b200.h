@@ -1,0 +1,141 @@
+/*
+ * mhd_b200 — C ABI of the B200 (sm_100a) GLM-MHD backend.
+ *
+ * This is the drop-in boundary for the reference's accelerator plug-in seam
+ * (include/mhd/gpu/device_solver.hpp in the reference project). Each entry point names the
+ * reference interface it replaces. Plain C types only: no C++ or torch types cross it, and no
+ * exception leaves it. Every call returns an mhdb_status; the message of the last failure on a
+ * handle is available from mhdb_last_error().
+ *
+ * State exchanged with the host uses the reference's StateField layout
+ * (include/state/state_field.hpp:9-73): nine planes (rho, mx, my, mz, E, bx, by, bz, psi), each
+ * (ny + 2 ng) x (nx + 2 ng) doubles, row-major, including ghost cells. On the device the state
+ * lives without ghosts in padded SoA planes; boundary conditions are applied as index maps when
+ * tiles are loaded.
+ *
+ * Threading: one handle per host thread at a time. All work of a handle runs on its own CUDA
+ * stream on the device that was current when the handle was created.
+ */
+#ifndef MHD_B200_H
+#define MHD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MHDB_OK = 0,
+    MHDB_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+    MHDB_MAX_STEPS = 2,        /* "solve: reached max_steps before t_end" */
+    MHDB_CUDA_ERROR = 3,       /* std::runtime_error("CUDA: ...") */
+    MHDB_NO_DEVICE = 4,        /* factory: no CUDA device */
+    MHDB_BAD_TIMESTEP = 5      /* dt not positive (ssp_rk2_step's invalid_argument) */
+} mhdb_status;
+
+/* Precision (reference: enum class Precision, device_solver.hpp:28). FP32 selects the
+   FP32-mixed form: FP32 arithmetic with the state carried as a compensated hi/lo pair. */
+enum { MHDB_FP64 = 0, MHDB_FP32 = 1 };
+
+/* Boundary types, same numbering as the reference's BoundaryConditionType
+   (include/boundary_conditions/boundary_conditions.hpp:8). Reflective is rejected, as in the
+   reference. */
+enum { MHDB_BC_PERIODIC = 0, MHDB_BC_REFLECTIVE = 1, MHDB_BC_OUTFLOW = 2 };
+
+/* Slope limiters: SlopeLimiter::Minmod / MC (include/mhd/mhd_types.hpp:44) plus van Leer. */
+enum { MHDB_MINMOD = 0, MHDB_MC = 1, MHDB_VANLEER = 2 };
+
+/* Grid2D (include/grid/grid.hpp:5-26). */
+typedef struct {
+    int nx, ny, ng;
+    double x_min, x_max, y_min, y_max;
+} mhdb_grid;
+
+/* SolveParams with its NonIdealConfig flattened (include/mhd/solve_types.hpp:8-16,
+   include/physics_config/mhd_config.hpp:13-20). */
+typedef struct {
+    double t_end, cfl, gamma, glm_alpha;
+    int limiter;
+    int ohmic, hall, ambipolar;
+    double eta_ohm, eta_hall, eta_ambipolar;
+    int max_steps;
+} mhdb_params;
+
+/* SolveResult (include/mhd/solve_types.hpp:18-22). */
+typedef struct {
+    double t;
+    int steps;
+    double c_h;
+} mhdb_result;
+
+/* FP64 interior diagnostics: sums of rho*dx*dy and E*dx*dy, central-difference div B
+   (max and root-mean-square), minimum rho and p, and whether every value is finite. */
+typedef struct {
+    double mass, energy, div_b_max, div_b_l2, rho_min, p_min;
+    int finite;
+} mhdb_diag;
+
+typedef struct mhdb_solver mhdb_solver;
+
+/* mhd::cuda_available() (device_solver.hpp:78): 1 when a CUDA device is usable. */
+int mhdb_cuda_available(void);
+
+/* mhd::make_cuda_solver(grid, precision) (device_solver.hpp:82). Fails with
+   MHDB_INVALID_ARGUMENT when ng < 2 or the sizes are not positive, MHDB_NO_DEVICE without a
+   device. On failure *out is NULL and mhdb_last_error(NULL) holds the message. */
+int mhdb_create(const mhdb_grid* grid, int precision, mhdb_solver** out);
+
+/* ~DeviceSolver(). NULL is accepted. */
+void mhdb_destroy(mhdb_solver* h);
+
+/* Message of the last failure on h (h == NULL: of the last failed mhdb_create on this thread). */
+const char* mhdb_last_error(const mhdb_solver* h);
+
+/* DeviceSolver::device_name() (device_solver.hpp:62), e.g. "CUDA: NVIDIA B200". */
+int mhdb_device_name(const mhdb_solver* h, char* buf, size_t len);
+
+/* DeviceSolver::precision() (device_solver.hpp:63). */
+int mhdb_precision(const mhdb_solver* h);
+
+/* DeviceSolver::configure(bc, mask, reflective_walls) (device_solver.hpp:66-67). mask is the
+   interior fluid mask, row-major ny * nx bytes (1 = fluid), or NULL for all fluid; mask_len must
+   then be 0 or nx * ny. */
+int mhdb_configure(mhdb_solver* h, int bc_x, int bc_y, const uint8_t* mask, size_t mask_len,
+                   int reflective_walls);
+
+/* DeviceSolver::upload / download (device_solver.hpp:70-71): nine host planes of n_tot =
+   (nx + 2 ng)(ny + 2 ng) doubles each. download returns the state with ghosts filled by the
+   boundary rule and solid cells wall-filled, as the reference's solve() leaves it. */
+int mhdb_upload(mhdb_solver* h, const double* const comps[9], size_t n_tot);
+int mhdb_download(mhdb_solver* h, double* const comps[9], size_t n_tot);
+
+/* DeviceSolver::solve(params) (device_solver.hpp:73-74): advances the device state by
+   params->t_end (relative), same contract as the reference solve(). */
+int mhdb_solve(mhdb_solver* h, const mhdb_params* params, mhdb_result* result);
+
+/* Additive: advance exactly nsteps SSP-RK2 steps (no t_end limit; params->t_end is ignored). */
+int mhdb_solve_steps(mhdb_solver* h, const mhdb_params* params, int nsteps, mhdb_result* result);
+
+/* Additive: FP64 diagnostics of the device state (gamma from params). */
+int mhdb_diagnostics(mhdb_solver* h, const mhdb_params* params, mhdb_diag* out);
+
+/* Additive: the handle's CUDA stream (a cudaStream_t) for event timing by the caller. */
+void* mhdb_stream(mhdb_solver* h);
+
+/* Additive: per-kernel event timing. While enabled, every stage kernel launch is bracketed by
+   events (no CUDA graphs); mhdb_profile_read returns the summed milliseconds and launch counts
+   of the two stage kernels since the last reset. */
+int mhdb_set_profiling(mhdb_solver* h, int enabled);
+int mhdb_profile_read(mhdb_solver* h, double* ms_stage1, int* n_stage1, double* ms_stage2,
+                      int* n_stage2, int reset);
+
+/* Additive: number of kernel launches this handle has issued (graph nodes included). */
+long long mhdb_launch_count(const mhdb_solver* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,14 @@
+"""B200-native (sm_100a) backend for the 2D GLM-MHD finite-volume operator.
+
+* ``mhd_gpu_solver_b200.mhd_solver``: the reference's ``mhd_solver`` Python surface
+  (MHDSolver, SolveParams, NonIdealConfig, ...) running on the CUDA backend.
+* ``mhd_gpu_solver_b200._capi``: ctypes binding of the C ABI (include/mhd_b200.h).
+* ``mhd_gpu_solver_b200.workloads``: seeded synthetic initial states and masks.
+
+Importing the package loads ``libmhd_b200.so``; there is no CPU fallback, so the import fails
+with ImportError when the library has not been built.
+"""
+
+from . import _capi  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
+
+__all__ = ["_capi", "mhd_solver", "workloads"]

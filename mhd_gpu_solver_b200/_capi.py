@@ -1,0 +1,231 @@
+"""ctypes binding of the C ABI in ``include/mhd_b200.h``.
+
+The CUDA library is required: importing this module loads ``libmhd_b200.so`` and raises
+``ImportError`` if it has not been built. Status codes become the exception types the reference
+pybind module raises for the same C++ exceptions (std::invalid_argument -> ValueError,
+std::runtime_error -> RuntimeError).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmhd_b200.so")
+
+OK, INVALID_ARGUMENT, MAX_STEPS, CUDA_ERROR, NO_DEVICE, BAD_TIMESTEP = range(6)
+FP64, FP32 = 0, 1
+BC_PERIODIC, BC_REFLECTIVE, BC_OUTFLOW = 0, 1, 2
+MINMOD, MC, VANLEER = 0, 1, 2
+
+# Every entry point declared in include/mhd_b200.h.
+EXPORTS = (
+    "mhdb_cuda_available", "mhdb_create", "mhdb_destroy", "mhdb_last_error", "mhdb_device_name",
+    "mhdb_precision", "mhdb_configure", "mhdb_upload", "mhdb_download", "mhdb_solve",
+    "mhdb_solve_steps", "mhdb_diagnostics", "mhdb_stream", "mhdb_set_profiling",
+    "mhdb_profile_read", "mhdb_launch_count",
+)
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("ng", C.c_int), ("x_min", C.c_double),
+                ("x_max", C.c_double), ("y_min", C.c_double), ("y_max", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("t_end", C.c_double), ("cfl", C.c_double), ("gamma", C.c_double),
+                ("glm_alpha", C.c_double), ("limiter", C.c_int), ("ohmic", C.c_int),
+                ("hall", C.c_int), ("ambipolar", C.c_int), ("eta_ohm", C.c_double),
+                ("eta_hall", C.c_double), ("eta_ambipolar", C.c_double),
+                ("max_steps", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("t", C.c_double), ("steps", C.c_int), ("c_h", C.c_double)]
+
+
+class Diag(C.Structure):
+    _fields_ = [("mass", C.c_double), ("energy", C.c_double), ("div_b_max", C.c_double),
+                ("div_b_l2", C.c_double), ("rho_min", C.c_double), ("p_min", C.c_double),
+                ("finite", C.c_int)]
+
+
+_PD = C.POINTER(C.c_double)
+_PPD = C.POINTER(_PD)
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA backend first "
+            "(python -m mhd_gpu_solver_b200.build or __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    h = C.c_void_p
+    sig = {
+        "mhdb_cuda_available": ([], C.c_int),
+        "mhdb_create": ([C.POINTER(Grid), C.c_int, C.POINTER(h)], C.c_int),
+        "mhdb_destroy": ([h], None),
+        "mhdb_last_error": ([h], C.c_char_p),
+        "mhdb_device_name": ([h, C.c_char_p, C.c_size_t], C.c_int),
+        "mhdb_precision": ([h], C.c_int),
+        "mhdb_configure": ([h, C.c_int, C.c_int, C.POINTER(C.c_uint8), C.c_size_t, C.c_int],
+                           C.c_int),
+        "mhdb_upload": ([h, _PPD, C.c_size_t], C.c_int),
+        "mhdb_download": ([h, _PPD, C.c_size_t], C.c_int),
+        "mhdb_solve": ([h, C.POINTER(Params), C.POINTER(Result)], C.c_int),
+        "mhdb_solve_steps": ([h, C.POINTER(Params), C.c_int, C.POINTER(Result)], C.c_int),
+        "mhdb_diagnostics": ([h, C.POINTER(Params), C.POINTER(Diag)], C.c_int),
+        "mhdb_stream": ([h], C.c_void_p),
+        "mhdb_set_profiling": ([h, C.c_int], C.c_int),
+        "mhdb_profile_read": ([h, _PD, C.POINTER(C.c_int), _PD, C.POINTER(C.c_int), C.c_int],
+                              C.c_int),
+        "mhdb_launch_count": ([h], C.c_longlong),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+class MhdbError(RuntimeError):
+    """Failure reported through the C ABI; ``code`` is the mhdb_status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class MhdbValueError(ValueError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def raise_for(code: int, handle) -> None:
+    if code == OK:
+        return
+    msg = lib.mhdb_last_error(handle)
+    text = msg.decode() if msg else f"mhdb status {code}"
+    if code in (INVALID_ARGUMENT, BAD_TIMESTEP):
+        raise MhdbValueError(code, text)
+    raise MhdbError(code, text)
+
+
+def cuda_available() -> bool:
+    return bool(lib.mhdb_cuda_available())
+
+
+def plane_pointers(state: np.ndarray):
+    """Array of 9 double* into the planes of a C-contiguous (9, ny_tot, nx_tot) float64 array."""
+    if state.dtype != np.float64 or not state.flags.c_contiguous or state.shape[0] != 9:
+        raise ValueError("state must be a C-contiguous float64 array of shape (9, ny_tot, nx_tot)")
+    base = state.ctypes.data
+    stride = state.strides[0]
+    arr = (_PD * 9)(*[C.cast(C.c_void_p(base + c * stride), _PD) for c in range(9)])
+    return arr
+
+
+class DeviceSolver:
+    """Owning wrapper of one mhdb_solver handle (the reference DeviceSolver interface)."""
+
+    def __init__(self, nx: int, ny: int, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, ng=2,
+                 precision: int = FP64):
+        self._h = C.c_void_p()
+        g = Grid(int(nx), int(ny), int(ng), float(x_min), float(x_max), float(y_min),
+                 float(y_max))
+        raise_for(lib.mhdb_create(C.byref(g), int(precision), C.byref(self._h)), None)
+        self.nx, self.ny, self.ng = int(nx), int(ny), int(ng)
+        self.shape = (9, self.ny + 2 * self.ng, self.nx + 2 * self.ng)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.mhdb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_name(self) -> str:
+        buf = C.create_string_buffer(256)
+        raise_for(lib.mhdb_device_name(self._h, buf, 256), self._h)
+        return buf.value.decode()
+
+    def precision(self) -> int:
+        return lib.mhdb_precision(self._h)
+
+    def configure(self, bc_x: int, bc_y: int, mask=None, reflective_walls: bool = True) -> None:
+        if mask is None:
+            rc = lib.mhdb_configure(self._h, int(bc_x), int(bc_y), None, 0, int(reflective_walls))
+        else:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            rc = lib.mhdb_configure(self._h, int(bc_x), int(bc_y),
+                                    m.ctypes.data_as(C.POINTER(C.c_uint8)), m.size,
+                                    int(reflective_walls))
+        raise_for(rc, self._h)
+
+    def upload(self, state: np.ndarray) -> None:
+        ptrs = plane_pointers(state)
+        raise_for(lib.mhdb_upload(self._h, ptrs, state.shape[1] * state.shape[2]), self._h)
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float64)
+        ptrs = plane_pointers(out)
+        raise_for(lib.mhdb_download(self._h, ptrs, out.shape[1] * out.shape[2]), self._h)
+        return out
+
+    def solve(self, params: Params) -> Result:
+        r = Result()
+        raise_for(lib.mhdb_solve(self._h, C.byref(params), C.byref(r)), self._h)
+        return r
+
+    def solve_steps(self, params: Params, nsteps: int) -> Result:
+        r = Result()
+        raise_for(lib.mhdb_solve_steps(self._h, C.byref(params), int(nsteps), C.byref(r)),
+                  self._h)
+        return r
+
+    def diagnostics(self, params: Params) -> dict:
+        d = Diag()
+        raise_for(lib.mhdb_diagnostics(self._h, C.byref(params), C.byref(d)), self._h)
+        return {"mass": d.mass, "energy": d.energy, "div_b_max": d.div_b_max,
+                "div_b_l2": d.div_b_l2, "rho_min": d.rho_min, "p_min": d.p_min,
+                "finite": bool(d.finite)}
+
+    def stream(self) -> int:
+        return lib.mhdb_stream(self._h) or 0
+
+    def set_profiling(self, enabled: bool) -> None:
+        raise_for(lib.mhdb_set_profiling(self._h, int(enabled)), self._h)
+
+    def profile_read(self, reset: bool = True) -> dict:
+        m1, m2 = C.c_double(), C.c_double()
+        n1, n2 = C.c_int(), C.c_int()
+        raise_for(lib.mhdb_profile_read(self._h, C.byref(m1), C.byref(n1), C.byref(m2),
+                                        C.byref(n2), int(reset)), self._h)
+        return {"stage1_ms": m1.value, "stage1_launches": n1.value, "stage2_ms": m2.value,
+                "stage2_launches": n2.value}
+
+    def launch_count(self) -> int:
+        return int(lib.mhdb_launch_count(self._h))
+
+
+def make_params(t_end=0.0, cfl=0.4, gamma=5.0 / 3.0, glm_alpha=0.1, limiter=MC, ohmic=False,
+                hall=False, ambipolar=False, eta_ohm=0.0, eta_hall=0.0, eta_ambipolar=0.0,
+                max_steps=1_000_000) -> Params:
+    return Params(float(t_end), float(cfl), float(gamma), float(glm_alpha), int(limiter),
+                  int(bool(ohmic)), int(bool(hall)), int(bool(ambipolar)), float(eta_ohm),
+                  float(eta_hall), float(eta_ambipolar), int(max_steps))

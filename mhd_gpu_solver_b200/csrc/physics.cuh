@@ -1,0 +1,357 @@
+// Point-wise GLM-MHD numerics for the sm_100a stage kernels.
+//
+// Written for this project from the reference's numerical method; each function names the
+// reference file:line whose arithmetic (operation order included) it follows, so the FP64 form
+// agrees with the reference CPU path to round-off. All functions are templated on the
+// arithmetic type T (double for the plain form, float for the FP32-mixed form).
+#pragma once
+
+#include <cstdint>
+
+namespace mhdb {
+
+enum LimiterKind : int { kMinmod = 0, kMC = 1, kVanLeer = 2 };
+
+// Rotated frame: n = face normal, t = in-plane tangential (x-faces: n=x, t=y; y-faces: n=y,
+// t=x); include/mhd/kernels/muscl_hll.hpp:11-13,23-31.
+template <class T>
+struct PrimN {
+    T rho, vn, vt, vz, p, bn, bt, bz, psi;
+};
+
+template <class T>
+struct FluxN {
+    T rho, mn, mt, mz, e, bn, bt, bz, psi;
+};
+
+// mhd::simd scalar min/max (include/mhd/simd.hpp:40-47): the first operand wins ties and
+// NaN comparisons, exactly as (b < a) ? b : a.
+template <class T>
+__device__ __forceinline__ T vmin(T a, T b)
+{
+    return (b < a) ? b : a;
+}
+template <class T>
+__device__ __forceinline__ T vmax(T a, T b)
+{
+    return (a < b) ? b : a;
+}
+
+template <class T>
+__device__ __forceinline__ T tabs(T a)
+{
+    return a < T(0) ? -a : a;
+}
+
+// include/mhd/kernels/muscl_hll.hpp:33-38
+template <class T>
+__device__ __forceinline__ T minmod(T a, T b)
+{
+    return (a * b <= T(0)) ? T(0) : ((fabs(a) < fabs(b)) ? a : b);
+}
+
+// include/mhd/kernels/muscl_hll.hpp:41-47
+template <class T>
+__device__ __forceinline__ T mc_limiter(T a, T b)
+{
+    return minmod(T(0.5) * (a + b), minmod(T(2) * a, T(2) * b));
+}
+
+// van Leer (1974) harmonic limiter 2ab/(a+b) for same-sign slopes, else 0. The reference has
+// no van Leer limiter (include/mhd/mhd_types.hpp:44); this is the published formula.
+template <class T>
+__device__ __forceinline__ T vanleer_limiter(T a, T b)
+{
+    return (a * b <= T(0)) ? T(0) : (T(2) * a * b) / (a + b);
+}
+
+template <int L, class T>
+__device__ __forceinline__ T limit_slope(T a, T b)
+{
+    if constexpr (L == kMinmod) {
+        return minmod(a, b);
+    } else if constexpr (L == kMC) {
+        return mc_limiter(a, b);
+    } else {
+        return vanleer_limiter(a, b);
+    }
+}
+
+// Face i-1/2 from cells (i-2, i-1, i, i+1); include/mhd/kernels/muscl_hll.hpp:59-68.
+template <int L, class T>
+__device__ __forceinline__ void reconstruct(T wmm, T wm, T w0, T wp, T& left, T& right)
+{
+    const T dm = limit_slope<L>(wm - wmm, w0 - wm);
+    const T d0 = limit_slope<L>(w0 - wm, wp - w0);
+    left = wm + T(0.5) * dm;
+    right = w0 - T(0.5) * d0;
+}
+
+// Fast magnetosonic speed along n; include/mhd/kernels/muscl_hll.hpp:70-87.
+template <class T>
+__device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
+{
+    const T inv_rho = T(1) / W.rho;
+    const T cs2 = gamma * W.p * inv_rho;
+    const T bn2 = W.bn * W.bn;
+    const T b2 = bn2 + W.bt * W.bt + W.bz * W.bz;
+    const T va2 = b2 * inv_rho;
+    const T van2 = bn2 * inv_rho;
+    const T sum = cs2 + va2;
+    const T disc = vmax(sum * sum - T(4) * cs2 * van2, T(0));
+    const T cf2 = T(0.5) * (sum + sqrt(disc));
+    return sqrt(vmax(cf2, T(0)));
+}
+
+// Conserved state and GLM-MHD flux along n; include/mhd/kernels/muscl_hll.hpp:89-124.
+template <class T>
+__device__ __forceinline__ void conserved_and_flux(const PrimN<T>& W, T inv_gm1, T ch2,
+                                                   FluxN<T>& U, FluxN<T>& F)
+{
+    const T mn = W.rho * W.vn;
+    const T mt = W.rho * W.vt;
+    const T mz = W.rho * W.vz;
+    const T v2 = W.vn * W.vn + W.vt * W.vt + W.vz * W.vz;
+    const T b2 = W.bn * W.bn + W.bt * W.bt + W.bz * W.bz;
+    const T pmag = T(0.5) * b2;
+    const T energy = W.p * inv_gm1 + T(0.5) * W.rho * v2 + pmag;
+    const T pstar = W.p + pmag;
+    const T vb = W.vn * W.bn + W.vt * W.bt + W.vz * W.bz;
+
+    U.rho = W.rho;
+    U.mn = mn;
+    U.mt = mt;
+    U.mz = mz;
+    U.e = energy;
+    U.bn = W.bn;
+    U.bt = W.bt;
+    U.bz = W.bz;
+    U.psi = W.psi;
+
+    F.rho = mn;
+    F.mn = mn * W.vn + pstar - W.bn * W.bn;
+    F.mt = mn * W.vt - W.bn * W.bt;
+    F.mz = mn * W.vz - W.bn * W.bz;
+    F.e = (energy + pstar) * W.vn - W.bn * vb + W.psi * W.bn;
+    F.bn = W.psi;
+    F.bt = W.vn * W.bt - W.vt * W.bn;
+    F.bz = W.vn * W.bz - W.vz * W.bn;
+    F.psi = ch2 * W.bn;
+}
+
+// MUSCL + HLL with GLM wave bounds and the both-sides first-order fallback;
+// include/mhd/kernels/muscl_hll.hpp:126-209.
+template <int L, class T>
+__device__ __forceinline__ FluxN<T> muscl_hll_face(const PrimN<T>& Wmm, const PrimN<T>& Wm,
+                                                   const PrimN<T>& W0, const PrimN<T>& Wp,
+                                                   T gamma, T inv_gm1, T c_h)
+{
+    PrimN<T> WL, WR;
+    reconstruct<L>(Wmm.rho, Wm.rho, W0.rho, Wp.rho, WL.rho, WR.rho);
+    reconstruct<L>(Wmm.vn, Wm.vn, W0.vn, Wp.vn, WL.vn, WR.vn);
+    reconstruct<L>(Wmm.vt, Wm.vt, W0.vt, Wp.vt, WL.vt, WR.vt);
+    reconstruct<L>(Wmm.vz, Wm.vz, W0.vz, Wp.vz, WL.vz, WR.vz);
+    reconstruct<L>(Wmm.p, Wm.p, W0.p, Wp.p, WL.p, WR.p);
+    reconstruct<L>(Wmm.bn, Wm.bn, W0.bn, Wp.bn, WL.bn, WR.bn);
+    reconstruct<L>(Wmm.bt, Wm.bt, W0.bt, Wp.bt, WL.bt, WR.bt);
+    reconstruct<L>(Wmm.bz, Wm.bz, W0.bz, Wp.bz, WL.bz, WR.bz);
+    reconstruct<L>(Wmm.psi, Wm.psi, W0.psi, Wp.psi, WL.psi, WR.psi);
+
+    const T inf = T(INFINITY);
+    const bool ok = (WL.rho > T(0)) && (WL.p > T(0)) && (WL.rho < inf) && (WL.p < inf) &&
+                    (WR.rho > T(0)) && (WR.p > T(0)) && (WR.rho < inf) && (WR.p < inf);
+    if (!ok) {
+        WL = Wm;
+        WR = W0;
+    }
+
+    const T cfL = fast_speed_n(WL, gamma);
+    const T cfR = fast_speed_n(WR, gamma);
+    const T sL = vmin(vmin(WL.vn - cfL, WR.vn - cfR), -c_h);
+    const T sR = vmax(vmax(WL.vn + cfL, WR.vn + cfR), c_h);
+
+    const T ch2 = c_h * c_h;
+    FluxN<T> UL, UR, FL, FR;
+    conserved_and_flux(WL, inv_gm1, ch2, UL, FL);
+    conserved_and_flux(WR, inv_gm1, ch2, UR, FR);
+
+    const T denom = sR - sL;
+    const T inv_denom = T(1) / denom;
+    const T sLsR = sL * sR;
+    const bool use_left = sL >= T(0);
+    const bool use_right = sR <= T(0);
+    const bool degenerate = fabs(denom) < T(1.0e-14);
+
+    auto combine = [&](T fl, T fr, T ul, T ur) {
+        const T hll = (sR * fl - sL * fr + sLsR * (ur - ul)) * inv_denom;
+        const T mid = degenerate ? T(0.5) * (fl + fr) : hll;
+        return use_left ? fl : (use_right ? fr : mid);
+    };
+
+    FluxN<T> F;
+    F.rho = combine(FL.rho, FR.rho, UL.rho, UR.rho);
+    F.mn = combine(FL.mn, FR.mn, UL.mn, UR.mn);
+    F.mt = combine(FL.mt, FR.mt, UL.mt, UR.mt);
+    F.mz = combine(FL.mz, FR.mz, UL.mz, UR.mz);
+    F.e = combine(FL.e, FR.e, UL.e, UR.e);
+    F.bn = combine(FL.bn, FR.bn, UL.bn, UR.bn);
+    F.bt = combine(FL.bt, FR.bt, UL.bt, UR.bt);
+    F.bz = combine(FL.bz, FR.bz, UL.bz, UR.bz);
+    F.psi = combine(FL.psi, FR.psi, UL.psi, UR.psi);
+    return F;
+}
+
+// max(|vx| + cf_x, |vy| + cf_y) from conserved values; include/mhd/kernels/muscl_hll.hpp:211-239.
+template <class T>
+__device__ __forceinline__ T cell_max_signal_speed(T rho, T mx, T my, T mz, T energy, T bx, T by,
+                                                   T bz, T gamma)
+{
+    const T inv_rho = T(1) / rho;
+    PrimN<T> W;
+    W.rho = rho;
+    W.vn = mx * inv_rho;
+    W.vt = my * inv_rho;
+    W.vz = mz * inv_rho;
+    const T ekin = T(0.5) * (mx * mx + my * my + mz * mz) * inv_rho;
+    const T emag = T(0.5) * (bx * bx + by * by + bz * bz);
+    W.p = (gamma - T(1)) * (energy - ekin - emag);
+    W.bn = bx;
+    W.bt = by;
+    W.bz = bz;
+    W.psi = T(0);
+    const T sx = fabs(W.vn) + fast_speed_n(W, gamma);
+    PrimN<T> Wy = W;
+    Wy.vn = W.vt;
+    Wy.vt = W.vn;
+    Wy.bn = by;
+    Wy.bt = bx;
+    const T sy = fabs(Wy.vn) + fast_speed_n(Wy, gamma);
+    return vmax(sx, sy);
+}
+
+// Conserved -> primitive as the reference RHS does it (reciprocal of rho, then products);
+// include/mhd/kernels/cpu_rows.hpp:129-155. Writes rho, vx, vy, vz, p, bx, by, bz, psi.
+template <class T>
+__device__ __forceinline__ void cons_to_prim(const T* u, T gm1, T* w)
+{
+    const T rho = u[0], mx = u[1], my = u[2], mz = u[3], e = u[4];
+    const T bx = u[5], by = u[6], bz = u[7];
+    const T inv_rho = T(1) / rho;
+    const T ekin = T(0.5) * (mx * mx + my * my + mz * mz) * inv_rho;
+    const T emag = T(0.5) * (bx * bx + by * by + bz * bz);
+    w[0] = rho;
+    w[1] = mx * inv_rho;
+    w[2] = my * inv_rho;
+    w[3] = mz * inv_rho;
+    w[4] = gm1 * (e - ekin - emag);
+    w[5] = bx;
+    w[6] = by;
+    w[7] = bz;
+    w[8] = u[8];
+}
+
+// Reflective copy of one fluid neighbour into a solid cell: to_primitive (division form), negate
+// the normal velocity, floor rho and p at 1e-12, to_conservative;
+// include/mhd/mask.hpp:123-137 with include/mhd/mhd_physics.hpp:23-57. axis 0 = x neighbour.
+template <class T>
+__device__ __forceinline__ void reflect_fill(const T* s, int axis, T gm1, T* out)
+{
+    const T rho = s[0], mx = s[1], my = s[2], mz = s[3], E = s[4];
+    const T bx = s[5], by = s[6], bz = s[7];
+    T vx = mx / rho;
+    T vy = my / rho;
+    const T vz = mz / rho;
+    const T e_kin = T(0.5) * (mx * mx + my * my + mz * mz) / rho;
+    const T e_mag = T(0.5) * (bx * bx + by * by + bz * bz);
+    T p = gm1 * (E - e_kin - e_mag);
+    T r = rho;
+    if (axis == 0) {
+        vx = -vx;
+    } else {
+        vy = -vy;
+    }
+    if (r < T(1e-12)) {
+        r = T(1e-12);
+    }
+    if (p < T(1e-12)) {
+        p = T(1e-12);
+    }
+    const T ek = T(0.5) * r * (vx * vx + vy * vy + vz * vz);
+    const T em = T(0.5) * (bx * bx + by * by + bz * bz);
+    out[0] = r;
+    out[1] = r * vx;
+    out[2] = r * vy;
+    out[3] = r * vz;
+    out[4] = p / gm1 + ek + em;
+    out[5] = bx;
+    out[6] = by;
+    out[7] = bz;
+    out[8] = s[8];
+}
+
+// Benign state of a solid cell without fluid neighbours: rho = p = 1 at rest, zero B and psi
+// (include/mhd/mask.hpp:141-146).
+template <class T>
+__device__ __forceinline__ void isolated_fill(T gm1, T* out)
+{
+    out[0] = T(1);
+    out[1] = T(0);
+    out[2] = T(0);
+    out[3] = T(0);
+    out[4] = T(1) / gm1; // p / (gamma - 1) + 0 kinetic + 0 magnetic
+    out[5] = T(0);
+    out[6] = T(0);
+    out[7] = T(0);
+    out[8] = T(0);
+}
+
+// Generalised Ohm's law E = eta_O J + eta_H J x B / |B| + eta_A (J x B) x B / |B|^2, Hall and
+// ambipolar skipped where |B|^2 < 1e-14; include/mhd/nonideal.hpp:63-102.
+struct NonIdealCoef {
+    int ohmic, hall, ambipolar;
+    double eta_ohm, eta_hall, eta_ambipolar;
+};
+
+template <class T>
+__device__ __forceinline__ void nonideal_e(T Jx, T Jy, T Jz, T Bx, T By, T Bz,
+                                           const NonIdealCoef& c, T& Ex, T& Ey, T& Ez)
+{
+    Ex = T(0);
+    Ey = T(0);
+    Ez = T(0);
+    if (c.ohmic) {
+        const T eo = T(c.eta_ohm);
+        Ex += eo * Jx;
+        Ey += eo * Jy;
+        Ez += eo * Jz;
+    }
+    if (!(c.hall || c.ambipolar)) {
+        return;
+    }
+    const T B2 = Bx * Bx + By * By + Bz * Bz;
+    if (B2 < T(1.0e-14)) {
+        return;
+    }
+    const T cx = Jy * Bz - Jz * By;
+    const T cy = Jz * Bx - Jx * Bz;
+    const T cz = Jx * By - Jy * Bx;
+    if (c.hall) {
+        const T invB = T(1) / sqrt(B2);
+        const T eh = T(c.eta_hall);
+        Ex += eh * cx * invB;
+        Ey += eh * cy * invB;
+        Ez += eh * cz * invB;
+    }
+    if (c.ambipolar) {
+        const T dx = cy * Bz - cz * By;
+        const T dy = cz * Bx - cx * Bz;
+        const T dz = cx * By - cy * Bx;
+        const T invB2 = T(1) / B2;
+        const T ea = T(c.eta_ambipolar);
+        Ex += ea * dx * invB2;
+        Ey += ea * dy * invB2;
+        Ez += ea * dz * invB2;
+    }
+}
+
+} // namespace mhdb

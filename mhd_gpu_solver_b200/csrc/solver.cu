@@ -1,0 +1,932 @@
+// Host runtime of the B200 GLM-MHD backend and its C ABI (include/mhd_b200.h).
+//
+// One mhdb_solver owns, on the device that was current at creation:
+//   * the state U^n and the stage state U* as padded SoA planes without ghosts
+//     (FP64: 9 double planes each; FP32-mixed: 9 float hi + 9 float lo planes each),
+//   * the padded fluid mask, a device Ctrl block (FP64 clock, dt, c_h, step counter),
+//   * a ghosted staging buffer for host <-> device exchange in the reference layout,
+//   * one CUDA stream and cached CUDA graphs of batches of RK2 steps.
+// The time loop keeps dt on the device: each step is two launches (stage 1, stage 2 with the
+// CFL reduction fused in) and the host only polls Ctrl once per batch of steps, as the reference
+// CUDA backend does (src/cuda/cuda_solver.cu:601-655 in the reference project).
+
+#include "mhd_b200.h"
+
+#include "physics.cuh"
+#include "runtime_types.cuh"
+#include "stage_f64.cuh"
+#include "stage_mixed.cuh"
+#include "diagnostics.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+using namespace mhdb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaFail {
+    cudaError_t err;
+    const char* what;
+};
+
+#define MHDB_CHECK(expr)                                                                           \
+    do {                                                                                           \
+        const cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess) {                                                                   \
+            throw CudaFail{e_, #expr};                                                             \
+        }                                                                                          \
+    } while (0)
+
+struct ApiError {
+    int code;
+    std::string msg;
+};
+
+constexpr int kTileX64 = 32, kTileY64 = 8, kThreads64 = 256;
+constexpr int kTileXMx = 32, kTileYMx = 16, kThreadsMx = 256;
+constexpr int kInitThreads = 256;
+constexpr int kGraphBatch = 32;
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ---------------------------------------------------------------- pack / unpack kernels
+
+// Ghosted host layout (reference StateField) -> padded interior planes.
+__global__ void unpack_f64(const double* __restrict__ stg, double* __restrict__ u, Geometry g,
+                           int ng, int nxt, size_t ntot)
+{
+    const long long n = static_cast<long long>(g.nx) * g.ny;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        const size_t s = static_cast<size_t>(y + ng) * nxt + (x + ng);
+        const size_t d = static_cast<size_t>(y) * g.pitch + x;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            u[k * g.plane + d] = stg[k * ntot + s];
+        }
+    }
+}
+
+// Padded interior planes -> ghosted layout with the final ghost fill and wall fill of the
+// reference solve() (include/mhd/time_integrator.hpp:101-104): ghosts copy the (pre-fill)
+// stored value of the interior cell their boundary rule maps to; solid interior cells are
+// wall-filled.
+__global__ void pack_f64(const double* __restrict__ u, const uint8_t* __restrict__ mask,
+                         double* __restrict__ stg, Geometry g, int ng, int nxt, int nyt,
+                         size_t ntot, int fill, double gm1)
+{
+    const long long n = static_cast<long long>(nxt) * nyt;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(c % nxt), j = static_cast<int>(c / nxt);
+        const int gx = i - ng, gy = j - ng;
+        const int sx = map_index(gx, g.nx, g.bc_x), sy = map_index(gy, g.ny, g.bc_y);
+        const bool interior = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
+        double v[9];
+        if (fill && interior && is_solid(mask, g, sx, sy)) {
+            wall_fill_f64(u, mask, g, sx, sy, gm1, v);
+        } else {
+            load_cons_f64(u, g, sx, sy, v);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            stg[k * ntot + static_cast<size_t>(c)] = v[k];
+        }
+    }
+}
+
+// Wall fill of every solid interior cell in place. Reads fluid cells only and writes solid cells
+// only, so the order of cells does not matter (include/mhd/mask.hpp:85-149).
+__global__ void fill_solids_f64(double* __restrict__ u, const uint8_t* __restrict__ mask,
+                                Geometry g, double gm1)
+{
+    const long long n = static_cast<long long>(g.nx) * g.ny;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        if (!is_solid(mask, g, x, y)) {
+            continue;
+        }
+        double v[9];
+        wall_fill_f64(u, mask, g, x, y, gm1, v);
+        const size_t o = static_cast<size_t>(y) * g.pitch + x;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            u[k * g.plane + o] = v[k];
+        }
+    }
+}
+
+__global__ void fill_solids_mixed(MixedState u, const uint8_t* __restrict__ mask, Geometry g,
+                                  double gm1)
+{
+    const long long n = static_cast<long long>(g.nx) * g.ny;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        if (!is_solid(mask, g, x, y)) {
+            continue;
+        }
+        double v[9];
+        wall_fill_mx(u, mask, g, x, y, gm1, v);
+        const size_t o = static_cast<size_t>(y) * g.pitch + x;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            split_store(u, k * g.plane + o, v[k]);
+        }
+    }
+}
+
+using StageFnF64 = void (*)(StageArgsF64);
+
+template <int L, bool NI, bool MASK, int STAGE>
+StageFnF64 stage_fn_f64()
+{
+    return stage_kernel_f64<L, NI, MASK, STAGE, kTileX64, kTileY64, kThreads64>;
+}
+
+template <int L, bool NI, bool MASK>
+void stage_pair_f64(StageFnF64& s1, StageFnF64& s2)
+{
+    s1 = stage_fn_f64<L, NI, MASK, 1>();
+    s2 = stage_fn_f64<L, NI, MASK, 2>();
+}
+
+void select_f64(int lim, bool ni, bool mask, StageFnF64& s1, StageFnF64& s2)
+{
+#define MHDB_SEL(LL)                                                                               \
+    if (ni) {                                                                                      \
+        if (mask) stage_pair_f64<LL, true, true>(s1, s2);                                          \
+        else stage_pair_f64<LL, true, false>(s1, s2);                                              \
+    } else {                                                                                       \
+        if (mask) stage_pair_f64<LL, false, true>(s1, s2);                                         \
+        else stage_pair_f64<LL, false, false>(s1, s2);                                             \
+    }
+    if (lim == kMinmod) {
+        MHDB_SEL(kMinmod)
+    } else if (lim == kMC) {
+        MHDB_SEL(kMC)
+    } else {
+        MHDB_SEL(kVanLeer)
+    }
+#undef MHDB_SEL
+}
+
+struct Prof {
+    cudaEvent_t a, b;
+    int kind;
+};
+
+} // namespace
+
+struct mhdb_solver {
+    mhdb_grid grid{};
+    int precision = MHDB_FP64;
+    int device = 0;
+    std::string name;
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+
+    Geometry geom{};
+    int nxt = 0, nyt = 0;
+    size_t ntot = 0;
+
+    void* U = nullptr;  // U^n
+    void* Us = nullptr; // U*
+    double* staging = nullptr;
+    uint8_t* mask = nullptr;
+    Ctrl* ctrl = nullptr;
+    Ctrl* ctrl_host = nullptr;
+    double* diag = nullptr;      // kDiagFields * kDiagBlocks partials + kDiagFields results
+    double* diag_host = nullptr; // pinned copy of the results
+
+    bool has_mask = false;
+    bool walls = true;
+    // gamma - 1 of the last solve (the wall fill of download needs it) and whether the device
+    // state has been advanced since the last upload; an upload followed directly by a download
+    // returns the uploaded array unchanged, ghosts included.
+    double last_gm1 = 2.0 / 3.0;
+    bool solved_since_upload = false;
+
+    // graph cache for a batch of kGraphBatch steps
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<double> graph_key;
+
+    bool profiling = false;
+    std::vector<Prof> prof_pending;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pool;
+    size_t prof_used = 0;
+    double prof_ms[2] = {0.0, 0.0};
+    int prof_n[2] = {0, 0};
+    long long launches = 0;
+};
+
+namespace {
+
+int cuda_status(mhdb_solver* h, const CudaFail& f)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "CUDA: %s (%s)", cudaGetErrorString(f.err), f.what);
+    if (h != nullptr) {
+        h->last_error = buf;
+    } else {
+        g_create_error = buf;
+    }
+    return MHDB_CUDA_ERROR;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            prev = -1;
+        }
+        if (prev != dev) {
+            MHDB_CHECK(cudaSetDevice(dev));
+        }
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) {
+            cudaSetDevice(prev);
+        }
+    }
+};
+
+Consts make_consts(const mhdb_solver* h, const mhdb_params* p)
+{
+    Consts k{};
+    const double dx = (h->grid.x_max - h->grid.x_min) / static_cast<double>(h->grid.nx);
+    const double dy = (h->grid.y_max - h->grid.y_min) / static_cast<double>(h->grid.ny);
+    k.gamma = p->gamma;
+    k.gm1 = p->gamma - 1.0;
+    k.inv_gm1 = 1.0 / (p->gamma - 1.0);
+    k.glm_alpha = p->glm_alpha;
+    k.inv_dx = 1.0 / dx;
+    k.inv_dy = 1.0 / dy;
+    k.inv_2dx = 0.5 / dx;
+    k.inv_2dy = 0.5 / dy;
+    k.h = (dy < dx) ? dy : dx;
+    k.cfl = p->cfl;
+    double eta = 0.0;
+    auto vmx = [](double a, double b) { return (a < b) ? b : a; };
+    if (p->ohmic) eta = vmx(eta, std::fabs(p->eta_ohm));
+    if (p->hall) eta = vmx(eta, std::fabs(p->eta_hall));
+    if (p->ambipolar) eta = vmx(eta, std::fabs(p->eta_ambipolar));
+    k.eta_max = eta;
+    k.dt_diff = eta > 0.0 ? p->cfl * k.h * k.h / (2.0 * 2.0 * eta) : 0.0;
+    k.ni.ohmic = p->ohmic != 0;
+    k.ni.hall = p->hall != 0;
+    k.ni.ambipolar = p->ambipolar != 0;
+    k.ni.eta_ohm = p->eta_ohm;
+    k.ni.eta_hall = p->eta_hall;
+    k.ni.eta_ambipolar = p->eta_ambipolar;
+    k.ni_any = (p->ohmic && p->eta_ohm != 0.0) || (p->hall && p->eta_hall != 0.0) ||
+               (p->ambipolar && p->eta_ambipolar != 0.0);
+    return k;
+}
+
+void validate_params(const mhdb_params* p, bool time_based)
+{
+    if (p == nullptr) {
+        throw ApiError{MHDB_INVALID_ARGUMENT, "params must not be NULL"};
+    }
+    if (time_based && p->t_end < 0.0) {
+        throw ApiError{MHDB_INVALID_ARGUMENT, "t_end must be non-negative"};
+    }
+    if (p->cfl <= 0.0) {
+        throw ApiError{MHDB_INVALID_ARGUMENT, "CFL number must be positive"};
+    }
+    if (p->limiter < kMinmod || p->limiter > kVanLeer) {
+        throw ApiError{MHDB_INVALID_ARGUMENT, "unknown slope limiter"};
+    }
+}
+
+// Launch plan of one RK2 step for the current state and parameters.
+struct StepPlan {
+    bool mixed = false;
+    StageFnF64 s1 = nullptr, s2 = nullptr;
+    StageArgsF64 a1{}, a2{};
+    StageFnMx m1 = nullptr, m2 = nullptr;
+    StageArgsMx b1{}, b2{};
+    dim3 grid, block;
+    size_t smem = 0;
+    Consts k{};
+};
+
+StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
+{
+    StepPlan s;
+    s.k = make_consts(h, p);
+    const bool ni = s.k.ni_any != 0;
+    if (h->precision == MHDB_FP64) {
+        select_f64(p->limiter, ni, h->has_mask, s.s1, s.s2);
+        s.grid = dim3((h->grid.nx + kTileX64 - 1) / kTileX64, (h->grid.ny + kTileY64 - 1) / kTileY64);
+        s.block = dim3(kThreads64);
+        s.smem = ni ? stage_smem_bytes_f64<kTileX64, kTileY64, true>()
+                    : stage_smem_bytes_f64<kTileX64, kTileY64, false>();
+        const double* u = static_cast<const double*>(h->U);
+        const double* us = static_cast<const double*>(h->Us);
+        s.a1 = StageArgsF64{u, static_cast<double*>(h->Us), h->has_mask ? h->mask : nullptr,
+                            h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
+        s.a2 = StageArgsF64{us, static_cast<double*>(h->U), h->has_mask ? h->mask : nullptr,
+                            h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
+        MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(s.smem)));
+    } else {
+        s.mixed = true;
+        select_mixed(p->limiter, ni, h->has_mask, s.m1, s.m2);
+        s.grid = dim3((h->grid.nx + kTileXMx - 1) / kTileXMx, (h->grid.ny + kTileYMx - 1) / kTileYMx);
+        s.block = dim3(kThreadsMx);
+        s.smem = ni ? stage_smem_bytes_mixed<kTileXMx, kTileYMx, true>()
+                    : stage_smem_bytes_mixed<kTileXMx, kTileYMx, false>();
+        const MixedState u = mixed_view(h->U, h->geom);
+        const MixedState us = mixed_view(h->Us, h->geom);
+        s.b1 = StageArgsMx{u, us, h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
+                           h->walls ? 1 : 0};
+        s.b2 = StageArgsMx{us, u, h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
+                           h->walls ? 1 : 0};
+        MHDB_CHECK(cudaFuncSetAttribute(s.m1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.m2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(s.smem)));
+    }
+    return s;
+}
+
+void launch_stage(mhdb_solver* h, const StepPlan& s, int stage)
+{
+    if (!s.mixed) {
+        (stage == 1 ? s.s1 : s.s2)<<<s.grid, s.block, s.smem, h->stream>>>(stage == 1 ? s.a1 : s.a2);
+    } else {
+        (stage == 1 ? s.m1 : s.m2)<<<s.grid, s.block, s.smem, h->stream>>>(stage == 1 ? s.b1 : s.b2);
+    }
+    ++h->launches;
+}
+
+std::pair<cudaEvent_t, cudaEvent_t> prof_events(mhdb_solver* h)
+{
+    if (h->prof_used == h->prof_pool.size()) {
+        cudaEvent_t a, b;
+        MHDB_CHECK(cudaEventCreate(&a));
+        MHDB_CHECK(cudaEventCreate(&b));
+        h->prof_pool.emplace_back(a, b);
+    }
+    return h->prof_pool[h->prof_used++];
+}
+
+void launch_step_direct(mhdb_solver* h, const StepPlan& s)
+{
+    for (int stage = 1; stage <= 2; ++stage) {
+        if (h->profiling) {
+            auto ev = prof_events(h);
+            MHDB_CHECK(cudaEventRecord(ev.first, h->stream));
+            launch_stage(h, s, stage);
+            MHDB_CHECK(cudaEventRecord(ev.second, h->stream));
+            h->prof_pending.push_back(Prof{ev.first, ev.second, stage - 1});
+        } else {
+            launch_stage(h, s, stage);
+        }
+    }
+}
+
+// Identity of a captured batch: everything a stage launch depends on, field by field (no
+// struct padding enters the comparison).
+std::vector<double> plan_key(const mhdb_solver* h, const mhdb_params* p, const StepPlan& s)
+{
+    return {static_cast<double>(reinterpret_cast<uintptr_t>(h->U)),
+            static_cast<double>(reinterpret_cast<uintptr_t>(h->Us)),
+            static_cast<double>(s.mixed), static_cast<double>(p->limiter),
+            static_cast<double>(h->has_mask), static_cast<double>(h->walls),
+            static_cast<double>(h->geom.bc_x), static_cast<double>(h->geom.bc_y),
+            p->gamma, p->glm_alpha, p->cfl,
+            static_cast<double>(p->ohmic), static_cast<double>(p->hall),
+            static_cast<double>(p->ambipolar), p->eta_ohm, p->eta_hall, p->eta_ambipolar,
+            static_cast<double>(h->grid.nx), static_cast<double>(h->grid.ny),
+            h->grid.x_min, h->grid.x_max, h->grid.y_min, h->grid.y_max};
+}
+
+void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n)
+{
+    if (h->profiling || n < kGraphBatch) {
+        for (int i = 0; i < n; ++i) {
+            launch_step_direct(h, s);
+        }
+        MHDB_CHECK(cudaGetLastError());
+        return;
+    }
+    const std::vector<double> key = plan_key(h, p, s);
+    if (h->graph_exec == nullptr || key != h->graph_key) {
+        if (h->graph_exec != nullptr) {
+            cudaGraphExecDestroy(h->graph_exec);
+            h->graph_exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        MHDB_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = h->launches;
+        for (int i = 0; i < kGraphBatch; ++i) {
+            launch_step_direct(h, s);
+        }
+        h->launches = before;
+        const cudaError_t cap = cudaStreamEndCapture(h->stream, &graph);
+        if (cap != cudaSuccess) {
+            throw CudaFail{cap, "cudaStreamEndCapture"};
+        }
+        const cudaError_t ins = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ins != cudaSuccess) {
+            h->graph_exec = nullptr;
+            throw CudaFail{ins, "cudaGraphInstantiate"};
+        }
+        h->graph_key = key;
+    }
+    const int batches = n / kGraphBatch;
+    for (int b = 0; b < batches; ++b) {
+        MHDB_CHECK(cudaGraphLaunch(h->graph_exec, h->stream));
+        h->launches += 2 * kGraphBatch;
+    }
+    for (int i = 0; i < n - batches * kGraphBatch; ++i) {
+        launch_step_direct(h, s);
+    }
+    MHDB_CHECK(cudaGetLastError());
+}
+
+void start_solve(mhdb_solver* h, const StepPlan& s, double t_end, int max_steps)
+{
+    Ctrl c{};
+    c.t = 0.0;
+    c.dt = 0.0;
+    c.c_h = 0.0;
+    c.t_end = t_end;
+    c.ch_bits = 0ull;
+    c.arrived = 0u;
+    c.steps = 0;
+    c.max_steps = max_steps;
+    c.finished = 0;
+    c.status = 0;
+    *h->ctrl_host = c;
+    MHDB_CHECK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice,
+                               h->stream));
+    const long long ncell = static_cast<long long>(h->grid.nx) * h->grid.ny;
+    const int blocks = static_cast<int>(std::min<long long>((ncell + kInitThreads - 1) / kInitThreads, 148LL * 8));
+    if (!s.mixed) {
+        cfl_init_kernel_f64<kInitThreads><<<blocks, kInitThreads, 0, h->stream>>>(
+            static_cast<const double*>(h->U), h->mask, h->geom, s.k, h->ctrl, h->has_mask ? 1 : 0);
+    } else {
+        cfl_init_kernel_mixed<kInitThreads><<<blocks, kInitThreads, 0, h->stream>>>(
+            mixed_view(h->U, h->geom), h->mask, h->geom, s.k, h->ctrl, h->has_mask ? 1 : 0);
+    }
+    ++h->launches;
+    MHDB_CHECK(cudaGetLastError());
+}
+
+void read_ctrl(mhdb_solver* h)
+{
+    MHDB_CHECK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
+                               h->stream));
+    MHDB_CHECK(cudaStreamSynchronize(h->stream));
+}
+
+void ensure_staging(mhdb_solver* h)
+{
+    if (h->staging == nullptr) {
+        MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->staging), 9 * h->ntot * sizeof(double)));
+        MHDB_CHECK(cudaMemsetAsync(h->staging, 0, 9 * h->ntot * sizeof(double), h->stream));
+    }
+}
+
+int launch_blocks(long long n, int threads)
+{
+    return static_cast<int>(std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 16)));
+}
+
+template <class F>
+int guarded(mhdb_solver* h, F&& f)
+{
+    if (h == nullptr) {
+        g_create_error = "solver handle must not be NULL";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    try {
+        DeviceGuard dg(h->device);
+        f();
+        return MHDB_OK;
+    } catch (const ApiError& e) {
+        h->last_error = e.msg;
+        return e.code;
+    } catch (const CudaFail& e) {
+        return cuda_status(h, e);
+    } catch (const std::bad_alloc&) {
+        h->last_error = "out of host memory";
+        return MHDB_CUDA_ERROR;
+    }
+}
+
+void release(mhdb_solver* h)
+{
+    if (h->graph_exec != nullptr) cudaGraphExecDestroy(h->graph_exec);
+    for (auto& e : h->prof_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    if (h->U) cudaFree(h->U);
+    if (h->Us) cudaFree(h->Us);
+    if (h->staging) cudaFree(h->staging);
+    if (h->mask) cudaFree(h->mask);
+    if (h->ctrl) cudaFree(h->ctrl);
+    if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
+    if (h->diag) cudaFree(h->diag);
+    if (h->diag_host) cudaFreeHost(h->diag_host);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result* r)
+{
+    return guarded(h, [&] {
+        validate_params(p, fixed_steps < 0);
+        if (r == nullptr) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "result must not be NULL"};
+        }
+        const StepPlan s = make_plan(h, p);
+        if (h->solved_since_upload && h->has_mask && h->walls) {
+            // The state is the result of an earlier solve, which the reference leaves wall-filled
+            // (time_integrator.hpp:101-104); apply that fill now so that ghosts of solid edge
+            // cells see the filled values, as after a download/upload round trip.
+            const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+            if (h->precision == MHDB_FP64) {
+                fill_solids_f64<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                    static_cast<double*>(h->U), h->mask, h->geom, h->last_gm1);
+            } else {
+                fill_solids_mixed<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                    mixed_view(h->U, h->geom), h->mask, h->geom, h->last_gm1);
+            }
+            ++h->launches;
+            MHDB_CHECK(cudaGetLastError());
+        }
+        h->last_gm1 = p->gamma - 1.0;
+        h->solved_since_upload = true;
+        if (fixed_steps >= 0) {
+            start_solve(h, s, static_cast<double>(INFINITY), fixed_steps);
+            launch_steps(h, p, s, fixed_steps);
+            read_ctrl(h);
+        } else {
+            start_solve(h, s, p->t_end, p->max_steps);
+            // Batches of steps between host polls, sized from the observed dt
+            // (same policy as the reference CUDA backend: 4 first, then an estimate, <= 256).
+            int batch = 4;
+            double last_t = 0.0;
+            int last_steps = 0;
+            read_ctrl(h);
+            while (h->ctrl_host->finished == 0) {
+                batch = std::min(batch, std::max(1, p->max_steps - h->ctrl_host->steps));
+                launch_steps(h, p, s, batch);
+                read_ctrl(h);
+                const Ctrl& c = *h->ctrl_host;
+                if (c.finished != 0) {
+                    break;
+                }
+                const double dt_avg = c.steps > last_steps ? (c.t - last_t) / (c.steps - last_steps) : 0.0;
+                last_t = c.t;
+                last_steps = c.steps;
+                int est = batch * 2;
+                if (dt_avg > 0.0) {
+                    est = static_cast<int>(std::ceil((p->t_end - c.t) / dt_avg)) + 1;
+                }
+                batch = std::clamp(est, 1, 256);
+            }
+        }
+        const Ctrl& c = *h->ctrl_host;
+        if ((c.status & kStatusBadDt) != 0) {
+            throw ApiError{MHDB_BAD_TIMESTEP, "ssp_rk2_step requires positive dt"};
+        }
+        r->t = c.t;
+        r->steps = c.steps;
+        r->c_h = c.c_h;
+        if (fixed_steps < 0 && c.t < p->t_end) {
+            throw ApiError{MHDB_MAX_STEPS, "solve: reached max_steps before t_end"};
+        }
+    });
+}
+
+} // namespace
+
+extern "C" {
+
+int mhdb_cuda_available(void)
+{
+    int count = 0;
+    return (cudaGetDeviceCount(&count) == cudaSuccess && count > 0) ? 1 : 0;
+}
+
+int mhdb_create(const mhdb_grid* grid, int precision, mhdb_solver** out)
+{
+    if (out == nullptr || grid == nullptr) {
+        g_create_error = "grid and out must not be NULL";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (grid->ng < 2) {
+        g_create_error = "CUDA solver requires grid.ng >= 2";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    if (grid->nx < 1 || grid->ny < 1) {
+        g_create_error = "grid sizes must be positive";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    if (precision != MHDB_FP64 && precision != MHDB_FP32) {
+        g_create_error = "unknown precision";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    if (!mhdb_cuda_available()) {
+        g_create_error = "CUDA: no device available";
+        return MHDB_NO_DEVICE;
+    }
+    auto* h = new (std::nothrow) mhdb_solver();
+    if (h == nullptr) {
+        g_create_error = "out of host memory";
+        return MHDB_CUDA_ERROR;
+    }
+    h->grid = *grid;
+    h->precision = precision;
+    try {
+        MHDB_CHECK(cudaGetDevice(&h->device));
+        cudaDeviceProp prop{};
+        MHDB_CHECK(cudaGetDeviceProperties(&prop, h->device));
+        h->name = std::string("CUDA: ") + prop.name;
+        MHDB_CHECK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->nxt = grid->nx + 2 * grid->ng;
+        h->nyt = grid->ny + 2 * grid->ng;
+        h->ntot = static_cast<size_t>(h->nxt) * h->nyt;
+        h->geom.nx = grid->nx;
+        h->geom.ny = grid->ny;
+        h->geom.pitch = round_up(grid->nx, 32);
+        h->geom.bc_x = kPeriodic;
+        h->geom.bc_y = kPeriodic;
+        h->geom.plane = static_cast<size_t>(h->geom.pitch) * grid->ny;
+        const size_t bytes = 9 * h->geom.plane * 8; // FP64 or two FP32 halves
+        MHDB_CHECK(cudaMalloc(&h->U, bytes));
+        MHDB_CHECK(cudaMalloc(&h->Us, bytes));
+        MHDB_CHECK(cudaMemsetAsync(h->U, 0, bytes, h->stream));
+        MHDB_CHECK(cudaMemsetAsync(h->Us, 0, bytes, h->stream));
+        MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->mask), h->geom.plane));
+        MHDB_CHECK(cudaMemsetAsync(h->mask, 1, h->geom.plane, h->stream));
+        MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->ctrl), sizeof(Ctrl)));
+        MHDB_CHECK(cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), h->stream));
+        MHDB_CHECK(cudaMallocHost(reinterpret_cast<void**>(&h->ctrl_host), sizeof(Ctrl)));
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+    } catch (const CudaFail& e) {
+        cuda_status(nullptr, e);
+        release(h);
+        delete h;
+        return MHDB_CUDA_ERROR;
+    }
+    *out = h;
+    return MHDB_OK;
+}
+
+void mhdb_destroy(mhdb_solver* h)
+{
+    if (h == nullptr) {
+        return;
+    }
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        release(h);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    delete h;
+}
+
+const char* mhdb_last_error(const mhdb_solver* h)
+{
+    return h == nullptr ? g_create_error.c_str() : h->last_error.c_str();
+}
+
+int mhdb_device_name(const mhdb_solver* h, char* buf, size_t len)
+{
+    if (h == nullptr || buf == nullptr || len == 0) {
+        return MHDB_INVALID_ARGUMENT;
+    }
+    std::snprintf(buf, len, "%s", h->name.c_str());
+    return MHDB_OK;
+}
+
+int mhdb_precision(const mhdb_solver* h)
+{
+    return h == nullptr ? -1 : h->precision;
+}
+
+int mhdb_configure(mhdb_solver* h, int bc_x, int bc_y, const uint8_t* mask, size_t mask_len,
+                   int reflective_walls)
+{
+    return guarded(h, [&] {
+        if (bc_x == kReflective || bc_y == kReflective) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "Reflective boundary conditions are not implemented yet"};
+        }
+        if ((bc_x != kPeriodic && bc_x != kOutflow) || (bc_y != kPeriodic && bc_y != kOutflow)) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "unknown boundary condition type"};
+        }
+        const size_t n = static_cast<size_t>(h->grid.nx) * h->grid.ny;
+        bool active = false;
+        if (mask != nullptr) {
+            if (mask_len != n) {
+                throw ApiError{MHDB_INVALID_ARGUMENT, "FluidMask size does not match Grid2D interior"};
+            }
+            for (size_t i = 0; i < n && !active; ++i) {
+                active = mask[i] == 0;
+            }
+        }
+        h->geom.bc_x = bc_x;
+        h->geom.bc_y = bc_y;
+        h->walls = reflective_walls != 0;
+        h->has_mask = active;
+        if (active) {
+            MHDB_CHECK(cudaMemcpy2DAsync(h->mask, h->geom.pitch, mask, h->grid.nx, h->grid.nx,
+                                         h->grid.ny, cudaMemcpyHostToDevice, h->stream));
+            MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        }
+    });
+}
+
+int mhdb_upload(mhdb_solver* h, const double* const comps[9], size_t n_tot)
+{
+    return guarded(h, [&] {
+        if (comps == nullptr || n_tot != h->ntot) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "StateField size does not match Grid2D"};
+        }
+        ensure_staging(h);
+        for (int c = 0; c < 9; ++c) {
+            if (comps[c] == nullptr) {
+                throw ApiError{MHDB_INVALID_ARGUMENT, "state component must not be NULL"};
+            }
+            MHDB_CHECK(cudaMemcpyAsync(h->staging + c * h->ntot, comps[c], h->ntot * sizeof(double),
+                                       cudaMemcpyHostToDevice, h->stream));
+        }
+        const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+        if (h->precision == MHDB_FP64) {
+            unpack_f64<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                h->staging, static_cast<double*>(h->U), h->geom, h->grid.ng, h->nxt, h->ntot);
+        } else {
+            unpack_mixed<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                h->staging, mixed_view(h->U, h->geom), h->geom, h->grid.ng, h->nxt, h->ntot);
+        }
+        ++h->launches;
+        MHDB_CHECK(cudaGetLastError());
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        h->solved_since_upload = false;
+    });
+}
+
+int mhdb_download(mhdb_solver* h, double* const comps[9], size_t n_tot)
+{
+    return guarded(h, [&] {
+        if (comps == nullptr || n_tot != h->ntot) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "StateField size does not match Grid2D"};
+        }
+        ensure_staging(h);
+        // gamma only matters for the wall fill; it is the one of the last solve.
+        const double gm1 = h->last_gm1;
+        const long long n = static_cast<long long>(h->ntot);
+        const int fill = (h->has_mask && h->walls) ? 1 : 0;
+        if (!h->solved_since_upload) {
+            // staging still holds the uploaded array
+        } else if (h->precision == MHDB_FP64) {
+            pack_f64<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                static_cast<const double*>(h->U), h->mask, h->staging, h->geom, h->grid.ng, h->nxt,
+                h->nyt, h->ntot, fill, gm1);
+        } else {
+            pack_mixed<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                mixed_view(h->U, h->geom), h->mask, h->staging, h->geom, h->grid.ng, h->nxt,
+                h->nyt, h->ntot, fill, gm1);
+        }
+        if (h->solved_since_upload) {
+            ++h->launches;
+        }
+        MHDB_CHECK(cudaGetLastError());
+        for (int c = 0; c < 9; ++c) {
+            if (comps[c] == nullptr) {
+                throw ApiError{MHDB_INVALID_ARGUMENT, "state component must not be NULL"};
+            }
+            MHDB_CHECK(cudaMemcpyAsync(comps[c], h->staging + c * h->ntot, h->ntot * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->stream));
+        }
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int mhdb_solve(mhdb_solver* h, const mhdb_params* params, mhdb_result* result)
+{
+    return run_solve(h, params, -1, result);
+}
+
+int mhdb_solve_steps(mhdb_solver* h, const mhdb_params* params, int nsteps, mhdb_result* result)
+{
+    if (nsteps < 0) {
+        if (h != nullptr) h->last_error = "nsteps must be non-negative";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    return run_solve(h, params, nsteps, result);
+}
+
+int mhdb_diagnostics(mhdb_solver* h, const mhdb_params* params, mhdb_diag* out)
+{
+    return guarded(h, [&] {
+        if (params == nullptr || out == nullptr) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "params and out must not be NULL"};
+        }
+        if (h->diag == nullptr) {
+            MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->diag),
+                                  sizeof(double) * kDiagFields * (kDiagBlocks + 1)));
+            MHDB_CHECK(cudaMallocHost(reinterpret_cast<void**>(&h->diag_host),
+                                      sizeof(double) * kDiagFields));
+        }
+        const Consts k = make_consts(h, params);
+        const double dx = (h->grid.x_max - h->grid.x_min) / static_cast<double>(h->grid.nx);
+        const double dy = (h->grid.y_max - h->grid.y_min) / static_cast<double>(h->grid.ny);
+        const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+        const int blocks = static_cast<int>(std::min<long long>(kDiagBlocks, (n + kDiagThreads - 1) / kDiagThreads));
+        const int fill = (h->has_mask && h->walls) ? 1 : 0;
+        if (h->precision == MHDB_FP64) {
+            diag_partial<<<blocks, kDiagThreads, 0, h->stream>>>(
+                DiagLoaderF64{static_cast<const double*>(h->U)}, h->mask, fill, h->geom, k.gm1,
+                k.inv_2dx, k.inv_2dy, h->diag);
+        } else {
+            diag_partial<<<blocks, kDiagThreads, 0, h->stream>>>(
+                DiagLoaderMx{mixed_view(h->U, h->geom)}, h->mask, fill, h->geom, k.gm1, k.inv_2dx,
+                k.inv_2dy, h->diag);
+        }
+        double* res = h->diag + kDiagFields * kDiagBlocks;
+        diag_final<<<1, 32, 0, h->stream>>>(h->diag, blocks, dx * dy, n, res);
+        h->launches += 2;
+        MHDB_CHECK(cudaGetLastError());
+        MHDB_CHECK(cudaMemcpyAsync(h->diag_host, res, sizeof(double) * kDiagFields,
+                                   cudaMemcpyDeviceToHost, h->stream));
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        out->mass = h->diag_host[0];
+        out->energy = h->diag_host[1];
+        out->div_b_max = h->diag_host[2];
+        out->div_b_l2 = h->diag_host[3];
+        out->rho_min = h->diag_host[4];
+        out->p_min = h->diag_host[5];
+        out->finite = h->diag_host[6] == 0.0 ? 1 : 0;
+    });
+}
+
+void* mhdb_stream(mhdb_solver* h)
+{
+    return h == nullptr ? nullptr : static_cast<void*>(h->stream);
+}
+
+int mhdb_set_profiling(mhdb_solver* h, int enabled)
+{
+    if (h == nullptr) return MHDB_INVALID_ARGUMENT;
+    h->profiling = enabled != 0;
+    return MHDB_OK;
+}
+
+int mhdb_profile_read(mhdb_solver* h, double* ms1, int* n1, double* ms2, int* n2, int reset)
+{
+    return guarded(h, [&] {
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        for (const Prof& p : h->prof_pending) {
+            float ms = 0.f;
+            MHDB_CHECK(cudaEventElapsedTime(&ms, p.a, p.b));
+            h->prof_ms[p.kind] += ms;
+            h->prof_n[p.kind] += 1;
+        }
+        h->prof_pending.clear();
+        h->prof_used = 0;
+        if (ms1) *ms1 = h->prof_ms[0];
+        if (n1) *n1 = h->prof_n[0];
+        if (ms2) *ms2 = h->prof_ms[1];
+        if (n2) *n2 = h->prof_n[1];
+        if (reset) {
+            h->prof_ms[0] = h->prof_ms[1] = 0.0;
+            h->prof_n[0] = h->prof_n[1] = 0;
+        }
+    });
+}
+
+long long mhdb_launch_count(const mhdb_solver* h)
+{
+    return h == nullptr ? 0 : h->launches;
+}
+
+} // extern "C"

@@ -1,0 +1,41 @@
+"""Shared helpers of the test suite: initial states in the reference layout and error norms."""
+
+from __future__ import annotations
+
+import numpy as np
+
+from mhd_gpu_solver_b200 import workloads as wl
+from oracle import oracle as orc
+
+
+def initial_state(prim: dict, gamma: float, bc=(orc.PERIODIC, orc.PERIODIC), mask=None,
+                  walls: bool = True, ng: int = 2) -> np.ndarray:
+    """Ghosted state as MHDSolver.set_primitives leaves it: to_conservative on the interior,
+    ghost fill, then the wall fill when a mask with solid cells is set
+    (include/mhd/solver_api.hpp:243-274 of the reference)."""
+    ny, nx = prim["rho"].shape
+    U = wl.embed(wl.to_conservative(prim, gamma), ng)
+    grid = orc.Grid(nx, ny, ng)
+    U = orc.apply_bc(U, grid, bc)
+    if mask is not None and walls and not np.all(mask != 0):
+        U = orc.wall_fill(U, grid, mask, gamma)
+    return U
+
+
+def interior(U: np.ndarray, ng: int = 2) -> np.ndarray:
+    return U[:, ng:U.shape[1] - ng, ng:U.shape[2] - ng]
+
+
+def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per-component relative L1 of a vs b over the interior (absolute where b is all zero)."""
+    ai, bi = interior(a), interior(b)
+    num = np.abs(ai - bi).reshape(9, -1).sum(axis=1)
+    den = np.abs(bi).reshape(9, -1).sum(axis=1)
+    return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)
+
+
+def rel_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    ai, bi = interior(a), interior(b)
+    num = np.abs(ai - bi).reshape(9, -1).max(axis=1)
+    den = np.abs(bi).reshape(9, -1).max(axis=1)
+    return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)
