@@ -1,0 +1,350 @@
+"""Throughput benchmark of the B200 GLM-MHD backend (one JSON line on rank 0).
+
+Workload: the smooth periodic Fourier state at 4096^2 (gamma 5/3, CFL 0.4, van Leer, ideal
+GLM-MHD), seeded synthetic input. A step is one SSP-RK2 step of the whole grid; the metric is
+zone-updates/s (interior cells x steps / device seconds).
+
+* ``value``: FP32-mixed form, state resident in HBM, K timed steps bracketed by CUDA events on
+  the solver's stream after W warm-up steps. The state (1.2 GB) is far larger than L2 (126 MB),
+  so no flush is needed between steps. ``fp64`` reports the plain FP64 form the same way.
+* ``e2e``: the same metric through the C ABI the way a caller uses it (MHDSolver.run): per call,
+  upload from pinned host memory, 500 RK2 steps, download to pinned host memory.
+* ``roofline``: the dominant stage kernel's algorithmic bytes per launch (9 fields x 8 B:
+  stage 1 reads U and writes U*, 144 B/cell; stage 2 reads U* and U and writes U, 216 B/cell;
+  360 B per zone-update) over its average event-timed duration, against the measured HBM copy
+  bandwidth.
+* ``cpu_baseline``: the reference CPU solver (SIMD + threads), compiled from the reference's
+  own headers into oracle/_ref, on all host cores, on a bounded number of steps of the same
+  4096^2 state (MC limiter: the reference has no van Leer).
+
+``--impl reference`` times that reference CPU solver alone as the reference arm.
+Multi-GPU: the operator does not shard (replicas only); each rank runs the same workload on its
+own GPU and the value is the sum over ranks divided by the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 4096
+SEED = 0
+GAMMA = 5.0 / 3.0
+E2E_STEPS = 500
+BYTES_STAGE = {1: 144.0, 2: 216.0}  # algorithmic bytes per interior cell per launch
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="fp64,fp32_mixed",
+                    help="comma-separated subset of fp64,fp32_mixed (profiling runs)")
+    return ap.parse_args()
+
+
+def initial_state(n: int) -> np.ndarray:
+    from mhd_gpu_solver_b200 import workloads as wl
+    from mhd_gpu_solver_b200.mhd_solver import apply_boundary_conditions
+
+    U = wl.embed(wl.to_conservative(wl.fourier_state(n, n, SEED), GAMMA))
+    apply_boundary_conditions(U, n, n, 2, 0, 0)
+    return U
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def time_form(dev, params, steps: int, warmup: int, n: int) -> dict:
+    """Warm-up, then K steps with per-launch events on the solver's stream."""
+    import torch
+
+    dev.solve_steps(params, warmup)
+    dev.set_profiling(True)
+    dev.profile_read(reset=True)
+    stream = torch.cuda.ExternalStream(dev.stream())
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    launches0 = dev.launch_count()
+    start.record(stream)
+    dev.solve_steps(params, steps)
+    end.record(stream)
+    torch.cuda.synchronize()
+    launches = dev.launch_count() - launches0
+    ms = start.elapsed_time(end)
+    prof = dev.profile_read(reset=True)
+    dev.set_profiling(False)
+    cells = float(n) * n
+    out = {"ms": ms, "zone_updates_per_s": cells * steps / (ms * 1e-3), "launches": launches,
+           "prof": prof}
+    for stg in (1, 2):
+        k = prof[f"stage{stg}_launches"]
+        avg = prof[f"stage{stg}_ms"] / k if k else float("nan")
+        out[f"stage{stg}_avg_ms"] = avg
+        out[f"stage{stg}_gbs"] = BYTES_STAGE[stg] * cells / (avg * 1e-3) / 1e9 if k else None
+    return out
+
+
+def e2e_form(dev, params, host: np.ndarray, calls: int, n: int) -> dict:
+    """upload (pinned host) -> 500 steps -> download (pinned host), timed on the stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(dev.stream())
+    dev.upload(host)
+    dev.solve_steps(params, 2)
+    dev.download(host)
+    total = 0.0
+    for _ in range(calls):
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        dev.upload(host)
+        dev.solve_steps(params, E2E_STEPS)
+        dev.download(host)
+        end.record(stream)
+        torch.cuda.synchronize()
+        total += start.elapsed_time(end)
+    nbytes = int(host.nbytes)
+    return {"value": float(n) * n * E2E_STEPS * calls / (total * 1e-3), "unit": "zone-updates/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "steps_per_call": E2E_STEPS, "calls": calls}
+
+
+def cpu_reference_rate(U: np.ndarray, n: int, steps: int) -> dict:
+    from oracle import oracle as orc
+
+    threads = os.cpu_count() or 1
+    orc.ref_set_threads(threads)
+    p = orc.Params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=orc.MC, max_steps=1,
+                   fixed_steps=True)
+    orc.solve(U, orc.Grid(n, n), p, impl="ref")  # warm-up (thread pool, page faults)
+    p.max_steps = steps
+    orc.solve(U, orc.Grid(n, n), p, impl="ref")
+    dt = orc.ref_last_loop_seconds()
+    return {"value": float(n) * n * steps / dt, "unit": "zone-updates/s", "cores": threads,
+            "kind": "reference", "simd": orc.ref_simd_backend(), "seconds": dt,
+            "sample": f"{steps} SSP-RK2 steps of the {n}^2 periodic Fourier state, MC limiter "
+                      f"(the reference has no van Leer), reference CPU solver with "
+                      f"{orc.ref_simd_backend()} and {threads} threads"}
+
+
+def run_reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+
+    n = args.n
+    if orc.ref_library_path() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built"}))
+        return
+    U = initial_state(n)
+    threads = os.cpu_count() or 1
+    orc.ref_set_threads(threads)
+    p = orc.Params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=orc.MC, max_steps=1,
+                   fixed_steps=True)
+    p.max_steps = max(1, args.warmup)
+    state, *_ = orc.solve(U, orc.Grid(n, n), p, impl="ref")
+    p.max_steps = args.steps
+    orc.solve(state, orc.Grid(n, n), p, impl="ref")
+    dt = orc.ref_last_loop_seconds()
+    value = float(n) * n * args.steps / dt
+    sample = (f"{args.steps} SSP-RK2 steps of the {n}^2 periodic Fourier state after "
+              f"{args.warmup} warm-up steps, step loop timed alone, MC limiter (no van Leer in "
+              f"the reference), {orc.ref_simd_backend()}, {threads} threads")
+    line = {"metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"fourier_periodic_{n}x{n}", "grid": [n, n],
+                       "limiter": "MC", "parallelism": "cpu-threads"},
+            "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from mhd_gpu_solver_b200 import _capi
+
+    n = args.n
+    U = initial_state(n)
+    host = torch.empty(U.shape, dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = U
+    params = _capi.make_params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=_capi.VANLEER)
+
+    results = {}
+    forms = [f for f in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32))
+             if f[0] in args.forms.split(",")]
+    for name, prec in forms:
+        dev = _capi.DeviceSolver(n, n, precision=prec)
+        dev.configure(_capi.BC_PERIODIC, _capi.BC_PERIODIC)
+        dev.upload(host)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if name == "fp32_mixed":
+            with ClockSampler(local) as clk:
+                r = time_form(dev, params, args.steps, args.warmup, n)
+            r["clocks"] = clk.summary()
+        else:
+            r = time_form(dev, params, args.steps, args.warmup, n)
+        if dist is not None:
+            t = torch.tensor([r["ms"]], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            r["ms_max"] = float(t.item())
+        else:
+            r["ms_max"] = r["ms"]
+        if name == "fp32_mixed" and args.e2e_calls > 0:
+            r["e2e"] = e2e_form(dev, params, host, args.e2e_calls, n)
+        dev.close()
+        results[name] = r
+    if "fp32_mixed" not in results or "fp64" not in results:
+        if rank == 0:  # profiling run: no JSON line
+            print(json.dumps({k: {kk: vv for kk, vv in v.items() if kk != "prof"}
+                              for k, v in results.items()}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    mixed = results["fp32_mixed"]
+    ms = mixed["ms_max"]
+    value = world * float(n) * n * args.steps / (ms * 1e-3)
+    peak, peak_kind = measured_hbm_peak()
+    dom = 2 if mixed["prof"]["stage2_ms"] >= mixed["prof"]["stage1_ms"] else 1
+    achieved = mixed[f"stage{dom}_gbs"]
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"fourier_periodic_{n}x{n}", "grid": [n, n], "form": "fp32_mixed",
+                   "limiter": "van Leer", "gamma": GAMMA, "cfl": 0.4, "seed": SEED,
+                   "parallelism": f"replicas{world}",
+                   "l2": "state 1.21 GB per buffer >> 126 MB L2, no flush"},
+        "fp64": {"value": world * float(n) * n * args.steps / (results["fp64"]["ms_max"] * 1e-3),
+                 "ms_per_step": results["fp64"]["ms_max"] / args.steps,
+                 "stage1_avg_ms": results["fp64"]["stage1_avg_ms"],
+                 "stage2_avg_ms": results["fp64"]["stage2_avg_ms"],
+                 "stage2_gbs": results["fp64"]["stage2_gbs"]},
+        "speedup_fp32_mixed_over_fp64": results["fp64"]["ms_max"] / ms,
+        "roofline": {"bound": "hbm", "kernel": f"stage{dom} (fp32_mixed)", "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "algorithmic_bytes_per_launch": BYTES_STAGE[dom] * n * n,
+                     "stage1_avg_ms": mixed["stage1_avg_ms"],
+                     "stage2_avg_ms": mixed["stage2_avg_ms"]},
+        "clocks": mixed["clocks"],
+        "e2e": mixed.get("e2e"),
+        "gpu_launches": mixed["launches"],
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference_rate(U, n, args.cpu_steps)
+        except (FileNotFoundError, OSError) as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -73,6 +73,63 @@ def build_ref(force: bool = False) -> list[str]:
     return out
 
 
+PKG_DIR = os.path.join(os.path.dirname(HERE), "mhd_gpu_solver_b200")
+ADAPTER = os.path.join(PKG_DIR, "csrc", "reference_backend.cpp")
+REPO_INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+
+def _build_info_header() -> str:
+    """Stand-in for the CMake-generated include/mhd/build_info.hpp of the reference (its
+    template include/mhd/build_info.hpp.in only defines build-provenance strings)."""
+    gen = os.path.join(REF_DIR, "generated", "mhd")
+    os.makedirs(gen, exist_ok=True)
+    path = os.path.join(gen, "build_info.hpp")
+    vals = {"COMPILER_ID": "GNU", "COMPILER_VERSION": "g++", "CXX_STANDARD": "20",
+            "CMAKE_VERSION": "none", "TYPE": "Release", "GIT_COMMIT": "unknown",
+            "SYSTEM_NAME": "Linux", "SYSTEM_PROCESSOR": "x86_64", "NATIVE_ARCH": "OFF",
+            "SANITIZERS": "OFF"}
+    text = "#pragma once\n" + "".join(f'#define MHD_BUILD_{k} "{v}"\n' for k, v in vals.items())
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as f:
+            f.write(text)
+    return os.path.dirname(gen)
+
+
+def build_ref_with_b200(force: bool = False) -> list[str]:
+    """The reference's own Python module (python/mhd_pybind.cpp) and GPU gate tool
+    (tools/mhd_backend_compare.cpp), compiled from their sources with -DMHD_HAS_CUDA=1 and the
+    B200 backend (mhd_gpu_solver_b200/csrc/reference_backend.cpp + libmhd_b200.so) as their
+    CUDA backend. No-op without the reference checkout or the CUDA library."""
+    lib = os.path.join(PKG_DIR, "libmhd_b200.so")
+    if not reference_available() or not os.path.exists(lib):
+        return []
+    import sysconfig
+
+    import pybind11
+
+    os.makedirs(REF_DIR, exist_ok=True)
+    inc = os.path.join(REFERENCE_ROOT, "include")
+    gen = _build_info_header()
+    common = ["g++", "-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-fno-trapping-math",
+              "-ffp-contract=fast", "-march=x86-64-v3", "-pthread", "-DMHD_HAS_CUDA=1",
+              "-I", inc, "-I", gen, "-I", REPO_INCLUDE]
+    link = ["-L", PKG_DIR, "-l:libmhd_b200.so", "-Wl,-rpath,$ORIGIN/../../mhd_gpu_solver_b200"]
+    outs = []
+    mod = os.path.join(REF_DIR, "mhd_solver" + sysconfig.get_config_var("EXT_SUFFIX"))
+    src_mod = os.path.join(REFERENCE_ROOT, "python", "mhd_pybind.cpp")
+    if force or _stale(mod, [src_mod, ADAPTER, lib]):
+        _run(common + ["-fPIC", "-shared", "-I", pybind11.get_include(),
+                       "-I", sysconfig.get_paths()["include"], src_mod, ADAPTER, "-o", mod] + link)
+    outs.append(mod)
+    gate = os.path.join(REF_DIR, "mhd_backend_compare")
+    src_gate = os.path.join(REFERENCE_ROOT, "tools", "mhd_backend_compare.cpp")
+    if force or _stale(gate, [src_gate, ADAPTER, lib]):
+        _run(common + [src_gate, ADAPTER, "-o", gate] + link)
+    outs.append(gate)
+    return outs
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_ref_with_b200(force="--force" in sys.argv))

@@ -127,6 +127,7 @@ def _lib(impl: str) -> C.CDLL:
         lib.mhdr_set_threads.argtypes = [C.c_int]
         lib.mhdr_set_threads.restype = C.c_int
         lib.mhdr_simd_backend.restype = C.c_char_p
+        lib.mhdr_last_loop_seconds.restype = C.c_double
     else:
         raise ValueError(impl)
     solve = getattr(lib, prefix + "solve")
@@ -248,6 +249,11 @@ def diagnostics(U: np.ndarray, grid: Grid, gamma: float) -> dict:
 
 def ref_set_threads(n: int) -> int:
     return _lib("ref").mhdr_set_threads(int(n))
+
+
+def ref_last_loop_seconds() -> float:
+    """Step-loop seconds of the last impl="ref" solve (copies and allocation excluded)."""
+    return float(_lib("ref").mhdr_last_loop_seconds())
 
 
 def ref_simd_backend() -> str:

@@ -24,6 +24,7 @@
 #include "state/state_field.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -89,9 +90,18 @@ void store_state(const StateField& S, double* U)
     }
 }
 
+// Wall-clock seconds of the step loop of the last mhdr_solve (state copies and workspace
+// allocation excluded), as tools/mhd_backend_compare.cpp times run().
+double g_loop_seconds = 0.0;
+
 } // namespace
 
 extern "C" {
+
+double mhdr_last_loop_seconds()
+{
+    return g_loop_seconds;
+}
 
 int mhdr_set_threads(int n)
 {
@@ -124,6 +134,7 @@ int mhdr_solve(const mhdo_grid* g, const mhdo_params* p, int bc_x, int bc_y, con
             mptr = &fm;
         }
         SolveResult r{};
+        const auto t0 = std::chrono::steady_clock::now();
         if (p->fixed_steps == 0) {
             r = solve(S, work, grid, bc, sp, mptr, reflective_walls != 0);
         } else {
@@ -145,6 +156,8 @@ int mhdr_solve(const mhdo_grid* g, const mhdo_params* p, int bc_x, int bc_y, con
                 apply_solid_wall_fill(S, grid, *active, sp.gamma);
             }
         }
+        g_loop_seconds =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         store_state(S, U);
         out->t = r.t;
         out->steps = r.steps;
