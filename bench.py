@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="fp64,fp32_mixed",
                     help="comma-separated subset of fp64,fp32_mixed (profiling runs)")
+    ap.add_argument("--tile-config", type=int, default=-1,
+                    help="stage-kernel tile configuration for both forms (-1: autotune)")
     return ap.parse_args()
 
 
@@ -272,8 +274,16 @@ def main():
     results = {}
     forms = [f for f in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32))
              if f[0] in args.forms.split(",")]
+    from mhd_gpu_solver_b200 import autotune
+
+    chosen = {}
     for name, prec in forms:
+        cfg = args.tile_config
+        if cfg < 0:
+            cfg = autotune.tune(prec, _capi.VANLEER, n, n)
+        chosen[name] = cfg
         dev = _capi.DeviceSolver(n, n, precision=prec)
+        dev.set_tile_config(cfg)
         dev.configure(_capi.BC_PERIODIC, _capi.BC_PERIODIC)
         dev.upload(host)
         if dist is not None:
@@ -318,6 +328,8 @@ def main():
                    "limiter": "van Leer", "gamma": GAMMA, "cfl": 0.4, "seed": SEED,
                    "parallelism": f"replicas{world}",
                    "l2": "state 1.21 GB per buffer >> 126 MB L2, no flush"},
+        "tile_configs": {k: next(c for c in _capi.tile_configs(p) if c["config"] == chosen[k])
+                         for k, p in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32))},
         "fp64": {"value": world * float(n) * n * args.steps / (results["fp64"]["ms_max"] * 1e-3),
                  "ms_per_step": results["fp64"]["ms_max"] / args.steps,
                  "stage1_avg_ms": results["fp64"]["stage1_avg_ms"],

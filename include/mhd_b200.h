@@ -134,6 +134,15 @@ int mhdb_profile_read(mhdb_solver* h, double* ms_stage1, int* n_stage1, double* 
 /* Additive: number of kernel launches this handle has issued (graph nodes included). */
 long long mhdb_launch_count(const mhdb_solver* h);
 
+/* Additive: tile configurations of the stage kernels. Configuration 0 (the default) serves every
+   solve; the others exist for ideal solves without a mask and are picked per grid size class by
+   the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes tile width, tile
+   height, threads per CTA and the minimum CTAs per SM of one configuration. */
+int mhdb_tile_config_count(int precision);
+int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
+                          int* min_blocks);
+int mhdb_set_tile_config(mhdb_solver* h, int config);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,8 @@ EXPORTS = (
     "mhdb_cuda_available", "mhdb_create", "mhdb_destroy", "mhdb_last_error", "mhdb_device_name",
     "mhdb_precision", "mhdb_configure", "mhdb_upload", "mhdb_download", "mhdb_solve",
     "mhdb_solve_steps", "mhdb_diagnostics", "mhdb_stream", "mhdb_set_profiling",
-    "mhdb_profile_read", "mhdb_launch_count",
+    "mhdb_profile_read", "mhdb_launch_count", "mhdb_tile_config_count", "mhdb_tile_config_info",
+    "mhdb_set_tile_config",
 )
 
 
@@ -60,7 +61,7 @@ def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"{LIB_PATH} is missing: build the CUDA backend first "
-            "(python -m mhd_gpu_solver_b200.build or __graft_entry__.build())")
+            "(python mhd_gpu_solver_b200/build.py or __graft_entry__.build())")
     lib = C.CDLL(LIB_PATH)
     h = C.c_void_p
     sig = {
@@ -82,6 +83,10 @@ def _load() -> C.CDLL:
         "mhdb_profile_read": ([h, _PD, C.POINTER(C.c_int), _PD, C.POINTER(C.c_int), C.c_int],
                               C.c_int),
         "mhdb_launch_count": ([h], C.c_longlong),
+        "mhdb_tile_config_count": ([C.c_int], C.c_int),
+        "mhdb_tile_config_info": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "mhdb_set_tile_config": ([h, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -221,6 +226,19 @@ class DeviceSolver:
 
     def launch_count(self) -> int:
         return int(lib.mhdb_launch_count(self._h))
+
+    def set_tile_config(self, config: int) -> None:
+        raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
+
+
+def tile_configs(precision: int) -> list[dict]:
+    out = []
+    for c in range(lib.mhdb_tile_config_count(int(precision))):
+        v = [C.c_int() for _ in range(4)]
+        raise_for(lib.mhdb_tile_config_info(int(precision), c, *[C.byref(x) for x in v]), None)
+        out.append({"config": c, "tile_x": v[0].value, "tile_y": v[1].value,
+                    "threads": v[2].value, "min_blocks": v[3].value})
+    return out
 
 
 def make_params(t_end=0.0, cfl=0.4, gamma=5.0 / 3.0, glm_alpha=0.1, limiter=MC, ohmic=False,

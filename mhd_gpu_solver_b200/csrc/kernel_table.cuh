@@ -1,0 +1,75 @@
+// Instantiation helpers shared by kernels_f64.cu and kernels_mixed.cu.
+#pragma once
+
+#include "stage_kernel.cuh"
+#include "stage_select.h"
+
+namespace mhdb {
+
+template <int TX_, int TY_, int NT_, int MINB_>
+struct TileCfg {
+    static constexpr int TX = TX_, TY = TY_, NT = NT_, MINB = MINB_;
+};
+
+template <class Policy, class Cfg, int L, bool NI, bool MASK>
+void fill_pair(StageKernels& k)
+{
+    using T = typename Policy::T;
+    auto s1 = stage_kernel<Policy, L, NI, MASK, 1, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>;
+    auto s2 = stage_kernel<Policy, L, NI, MASK, 2, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>;
+    if constexpr (sizeof(T) == 8) {
+        k.f64_stage1 = s1;
+        k.f64_stage2 = s2;
+    } else {
+        k.mx_stage1 = s1;
+        k.mx_stage2 = s2;
+    }
+    k.tile_x = Cfg::TX;
+    k.tile_y = Cfg::TY;
+    k.threads = Cfg::NT;
+    k.smem = stage_smem_bytes<T, Cfg::TX, Cfg::TY, NI>();
+}
+
+// Every (limiter, non-ideal, mask) combination for the default configuration.
+template <class Policy, class Cfg>
+StageKernels select_full(int lim, bool ni, bool mask)
+{
+    StageKernels k;
+#define MHDB_SEL(LL)                                                                               \
+    if (ni) {                                                                                      \
+        if (mask) fill_pair<Policy, Cfg, LL, true, true>(k);                                       \
+        else fill_pair<Policy, Cfg, LL, true, false>(k);                                           \
+    } else {                                                                                       \
+        if (mask) fill_pair<Policy, Cfg, LL, false, true>(k);                                      \
+        else fill_pair<Policy, Cfg, LL, false, false>(k);                                          \
+    }
+    if (lim == kMinmod) {
+        MHDB_SEL(kMinmod)
+    } else if (lim == kMC) {
+        MHDB_SEL(kMC)
+    } else {
+        MHDB_SEL(kVanLeer)
+    }
+#undef MHDB_SEL
+    return k;
+}
+
+// Ideal, unmasked kernels only (tuning configurations).
+template <class Policy, class Cfg>
+StageKernels select_ideal(int lim, bool ni, bool mask)
+{
+    StageKernels k;
+    if (ni || mask) {
+        return k;
+    }
+    if (lim == kMinmod) {
+        fill_pair<Policy, Cfg, kMinmod, false, false>(k);
+    } else if (lim == kMC) {
+        fill_pair<Policy, Cfg, kMC, false, false>(k);
+    } else {
+        fill_pair<Policy, Cfg, kVanLeer, false, false>(k);
+    }
+    return k;
+}
+
+} // namespace mhdb

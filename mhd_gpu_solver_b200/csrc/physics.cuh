@@ -139,32 +139,12 @@ __device__ __forceinline__ void conserved_and_flux(const PrimN<T>& W, T inv_gm1,
     F.psi = ch2 * W.bn;
 }
 
-// MUSCL + HLL with GLM wave bounds and the both-sides first-order fallback;
-// include/mhd/kernels/muscl_hll.hpp:126-209.
-template <int L, class T>
-__device__ __forceinline__ FluxN<T> muscl_hll_face(const PrimN<T>& Wmm, const PrimN<T>& Wm,
-                                                   const PrimN<T>& W0, const PrimN<T>& Wp,
-                                                   T gamma, T inv_gm1, T c_h)
+// HLL flux with Dedner GLM wave-speed bounds (-c_h, +c_h) from the two face states, with the
+// upwind and degenerate (|sR - sL| < 1e-14) branches; include/mhd/kernels/muscl_hll.hpp:170-208.
+template <class T>
+__device__ __forceinline__ FluxN<T> hll_flux(const PrimN<T>& WL, const PrimN<T>& WR, T gamma,
+                                             T inv_gm1, T c_h)
 {
-    PrimN<T> WL, WR;
-    reconstruct<L>(Wmm.rho, Wm.rho, W0.rho, Wp.rho, WL.rho, WR.rho);
-    reconstruct<L>(Wmm.vn, Wm.vn, W0.vn, Wp.vn, WL.vn, WR.vn);
-    reconstruct<L>(Wmm.vt, Wm.vt, W0.vt, Wp.vt, WL.vt, WR.vt);
-    reconstruct<L>(Wmm.vz, Wm.vz, W0.vz, Wp.vz, WL.vz, WR.vz);
-    reconstruct<L>(Wmm.p, Wm.p, W0.p, Wp.p, WL.p, WR.p);
-    reconstruct<L>(Wmm.bn, Wm.bn, W0.bn, Wp.bn, WL.bn, WR.bn);
-    reconstruct<L>(Wmm.bt, Wm.bt, W0.bt, Wp.bt, WL.bt, WR.bt);
-    reconstruct<L>(Wmm.bz, Wm.bz, W0.bz, Wp.bz, WL.bz, WR.bz);
-    reconstruct<L>(Wmm.psi, Wm.psi, W0.psi, Wp.psi, WL.psi, WR.psi);
-
-    const T inf = T(INFINITY);
-    const bool ok = (WL.rho > T(0)) && (WL.p > T(0)) && (WL.rho < inf) && (WL.p < inf) &&
-                    (WR.rho > T(0)) && (WR.p > T(0)) && (WR.rho < inf) && (WR.p < inf);
-    if (!ok) {
-        WL = Wm;
-        WR = W0;
-    }
-
     const T cfL = fast_speed_n(WL, gamma);
     const T cfR = fast_speed_n(WR, gamma);
     const T sL = vmin(vmin(WL.vn - cfL, WR.vn - cfR), -c_h);

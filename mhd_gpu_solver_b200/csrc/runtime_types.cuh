@@ -47,16 +47,6 @@ struct Ctrl {
     int pad;
 };
 
-struct StageArgsF64 {
-    const double* uin;   // stage input (U^n for stage 1, U* for stage 2)
-    double* out;         // U* (stage 1) or U^n updated in place (stage 2)
-    const uint8_t* mask; // padded fluid mask or nullptr
-    Ctrl* ctrl;
-    Geometry geom;
-    Consts k;
-    int walls;           // reflective wall fill of solid cells (MHDSolver walls_reflective)
-};
-
 // Boundary rule as an index map onto the interior (include/boundary_conditions/
 // boundary_conditions.hpp:26-88): periodic wraps modulo n (valid for any offset, also when
 // n < 2), outflow clamps to the nearest interior cell. Ghost (i, j) of the reference holds

@@ -17,6 +17,7 @@
 #include "stage_f64.cuh"
 #include "stage_mixed.cuh"
 #include "diagnostics.cuh"
+#include "stage_select.h"
 
 #include <cuda_runtime.h>
 
@@ -52,8 +53,6 @@ struct ApiError {
     std::string msg;
 };
 
-constexpr int kTileX64 = 32, kTileY64 = 8, kThreads64 = 256;
-constexpr int kTileXMx = 32, kTileYMx = 16, kThreadsMx = 256;
 constexpr int kInitThreads = 256;
 constexpr int kGraphBatch = 32;
 
@@ -74,6 +73,46 @@ __global__ void unpack_f64(const double* __restrict__ stg, double* __restrict__ 
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             u[k * g.plane + d] = stg[k * ntot + s];
+        }
+    }
+}
+
+__global__ void unpack_mixed(const double* __restrict__ stg, MixedState u, Geometry g, int ng,
+                             int nxt, size_t ntot)
+{
+    const long long n = static_cast<long long>(g.nx) * g.ny;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        const size_t s = static_cast<size_t>(y + ng) * nxt + (x + ng);
+        const size_t d = static_cast<size_t>(y) * g.pitch + x;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            split_store(u, q * g.plane + d, stg[q * ntot + s]);
+        }
+    }
+}
+
+__global__ void pack_mixed(const MixedState u, const uint8_t* __restrict__ mask,
+                           double* __restrict__ stg, Geometry g, int ng, int nxt, int nyt,
+                           size_t ntot, int fill, double gm1)
+{
+    const long long n = static_cast<long long>(nxt) * nyt;
+    for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < n;
+         c += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int i = static_cast<int>(c % nxt), j = static_cast<int>(c / nxt);
+        const int gx = i - ng, gy = j - ng;
+        const int sx = map_index(gx, g.nx, g.bc_x), sy = map_index(gy, g.ny, g.bc_y);
+        const bool interior = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
+        double v[9];
+        if (fill && interior && is_solid(mask, g, sx, sy)) {
+            wall_fill_mx(u, mask, g, sx, sy, gm1, v);
+        } else {
+            load_cons_mx(u, g, sx, sy, v);
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            stg[q * ntot + static_cast<size_t>(c)] = v[q];
         }
     }
 }
@@ -148,41 +187,6 @@ __global__ void fill_solids_mixed(MixedState u, const uint8_t* __restrict__ mask
     }
 }
 
-using StageFnF64 = void (*)(StageArgsF64);
-
-template <int L, bool NI, bool MASK, int STAGE>
-StageFnF64 stage_fn_f64()
-{
-    return stage_kernel_f64<L, NI, MASK, STAGE, kTileX64, kTileY64, kThreads64>;
-}
-
-template <int L, bool NI, bool MASK>
-void stage_pair_f64(StageFnF64& s1, StageFnF64& s2)
-{
-    s1 = stage_fn_f64<L, NI, MASK, 1>();
-    s2 = stage_fn_f64<L, NI, MASK, 2>();
-}
-
-void select_f64(int lim, bool ni, bool mask, StageFnF64& s1, StageFnF64& s2)
-{
-#define MHDB_SEL(LL)                                                                               \
-    if (ni) {                                                                                      \
-        if (mask) stage_pair_f64<LL, true, true>(s1, s2);                                          \
-        else stage_pair_f64<LL, true, false>(s1, s2);                                              \
-    } else {                                                                                       \
-        if (mask) stage_pair_f64<LL, false, true>(s1, s2);                                         \
-        else stage_pair_f64<LL, false, false>(s1, s2);                                             \
-    }
-    if (lim == kMinmod) {
-        MHDB_SEL(kMinmod)
-    } else if (lim == kMC) {
-        MHDB_SEL(kMC)
-    } else {
-        MHDB_SEL(kVanLeer)
-    }
-#undef MHDB_SEL
-}
-
 struct Prof {
     cudaEvent_t a, b;
     int kind;
@@ -223,6 +227,7 @@ struct mhdb_solver {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<double> graph_key;
 
+    int tile_config = 0; // index into the compiled tile configurations (0 = default)
     bool profiling = false;
     std::vector<Prof> prof_pending;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pool;
@@ -331,39 +336,43 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     StepPlan s;
     s.k = make_consts(h, p);
     const bool ni = s.k.ni_any != 0;
+    StageKernels sk{};
+    // Tuned configurations exist for ideal, unmasked solves only; others use configuration 0.
+    const int cfg = (ni || h->has_mask) ? 0 : h->tile_config;
     if (h->precision == MHDB_FP64) {
-        select_f64(p->limiter, ni, h->has_mask, s.s1, s.s2);
-        s.grid = dim3((h->grid.nx + kTileX64 - 1) / kTileX64, (h->grid.ny + kTileY64 - 1) / kTileY64);
-        s.block = dim3(kThreads64);
-        s.smem = ni ? stage_smem_bytes_f64<kTileX64, kTileY64, true>()
-                    : stage_smem_bytes_f64<kTileX64, kTileY64, false>();
+        sk = select_stage_f64(p->limiter, ni, h->has_mask, cfg);
+        s.s1 = sk.f64_stage1;
+        s.s2 = sk.f64_stage2;
         const double* u = static_cast<const double*>(h->U);
         const double* us = static_cast<const double*>(h->Us);
         s.a1 = StageArgsF64{u, static_cast<double*>(h->Us), h->has_mask ? h->mask : nullptr,
                             h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
         s.a2 = StageArgsF64{us, static_cast<double*>(h->U), h->has_mask ? h->mask : nullptr,
                             h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
-        MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(s.smem)));
-        MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(s.smem)));
     } else {
         s.mixed = true;
-        select_mixed(p->limiter, ni, h->has_mask, s.m1, s.m2);
-        s.grid = dim3((h->grid.nx + kTileXMx - 1) / kTileXMx, (h->grid.ny + kTileYMx - 1) / kTileYMx);
-        s.block = dim3(kThreadsMx);
-        s.smem = ni ? stage_smem_bytes_mixed<kTileXMx, kTileYMx, true>()
-                    : stage_smem_bytes_mixed<kTileXMx, kTileYMx, false>();
+        sk = select_stage_mixed(p->limiter, ni, h->has_mask, cfg);
+        s.m1 = sk.mx_stage1;
+        s.m2 = sk.mx_stage2;
         const MixedState u = mixed_view(h->U, h->geom);
         const MixedState us = mixed_view(h->Us, h->geom);
         s.b1 = StageArgsMx{u, us, h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
                            h->walls ? 1 : 0};
         s.b2 = StageArgsMx{us, u, h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
                            h->walls ? 1 : 0};
-        MHDB_CHECK(cudaFuncSetAttribute(s.m1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(s.smem)));
-        MHDB_CHECK(cudaFuncSetAttribute(s.m2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(s.smem)));
+    }
+    if (sk.smem == 0) {
+        throw ApiError{MHDB_INVALID_ARGUMENT, "no stage kernel for this configuration"};
+    }
+    s.grid = dim3((h->grid.nx + sk.tile_x - 1) / sk.tile_x, (h->grid.ny + sk.tile_y - 1) / sk.tile_y);
+    s.block = dim3(sk.threads);
+    s.smem = sk.smem;
+    if (!s.mixed) {
+        MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
+    } else {
+        MHDB_CHECK(cudaFuncSetAttribute(s.m1, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.m2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
     }
     return s;
 }
@@ -417,6 +426,7 @@ std::vector<double> plan_key(const mhdb_solver* h, const mhdb_params* p, const S
             static_cast<double>(p->ohmic), static_cast<double>(p->hall),
             static_cast<double>(p->ambipolar), p->eta_ohm, p->eta_hall, p->eta_ambipolar,
             static_cast<double>(h->grid.nx), static_cast<double>(h->grid.ny),
+            static_cast<double>(h->tile_config),
             h->grid.x_min, h->grid.x_max, h->grid.y_min, h->grid.y_max};
 }
 
@@ -927,6 +937,39 @@ int mhdb_profile_read(mhdb_solver* h, double* ms1, int* n1, double* ms2, int* n2
 long long mhdb_launch_count(const mhdb_solver* h)
 {
     return h == nullptr ? 0 : h->launches;
+}
+
+int mhdb_tile_config_count(int precision)
+{
+    return precision == MHDB_FP32 ? stage_config_count_mixed() : stage_config_count_f64();
+}
+
+int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
+                          int* min_blocks)
+{
+    if (config < 0 || config >= mhdb_tile_config_count(precision)) {
+        return MHDB_INVALID_ARGUMENT;
+    }
+    const TileConfigInfo t = precision == MHDB_FP32 ? stage_config_info_mixed(config)
+                                                    : stage_config_info_f64(config);
+    if (tile_x) *tile_x = t.tile_x;
+    if (tile_y) *tile_y = t.tile_y;
+    if (threads) *threads = t.threads;
+    if (min_blocks) *min_blocks = t.min_blocks;
+    return MHDB_OK;
+}
+
+int mhdb_set_tile_config(mhdb_solver* h, int config)
+{
+    if (h == nullptr) {
+        return MHDB_INVALID_ARGUMENT;
+    }
+    if (config < 0 || config >= mhdb_tile_config_count(h->precision)) {
+        h->last_error = "unknown tile configuration";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    h->tile_config = config;
+    return MHDB_OK;
 }
 
 } // extern "C"

@@ -1,0 +1,340 @@
+// Fused SSP-RK2 stage kernel shared by both precision forms.
+//
+// One CTA owns a TX x TY tile of interior cells; a stage is one pass over HBM:
+//   A. stage the tile plus its 2-cell halo of the 9 conserved fields into shared memory as
+//      primitives; boundary conditions are index maps (periodic wrap / outflow clamp) applied
+//      while loading, and solid cells are wall-filled from their fluid neighbours;
+//   B. (non-ideal) cell-centred current J = curl B on the tile plus a 1-cell ring;
+//   C. x sweep: every cell of the tile plus a 1-cell x ring limits its slope once per component
+//      into shared memory; then every x-face flux (HLL + GLM + non-ideal E) is evaluated once
+//      from the face states W(l) + s(l)/2 and W(r) - s(r)/2 of its two cells, and each owned
+//      cell keeps dF = F(i+1/2) - F(i-1/2) in registers;
+//   D. y sweep: the same for y, reusing the slope and flux buffers;
+//   E. L = -dF/dx - dG/dy, Dedner psi damping, L = 0 on solids, and the stage update
+//      (stage 1: U* = U + dt L; stage 2: U = (U + U*)/2 + (dt/2) L, written in place);
+//   F. stage 2 reduces the next step's max signal speed (warp shuffles, one 64-bit atomic max
+//      per CTA) and the last CTA to arrive turns it into the next dt (FP64 clock).
+//
+// Per-cell slopes give the same values as the reference's per-face reconstruction
+// (include/mhd/kernels/muscl_hll.hpp:59-68): the left state of face i-1/2 is
+// W(i-1) + lim(W(i-1) - W(i-2), W(i) - W(i-1))/2, built from cell i-1's slope, and the right
+// state W(i) - lim(W(i) - W(i-1), W(i+1) - W(i))/2 from cell i's slope; each slope is limited
+// once instead of once per adjacent face, with the same operations on the same operands.
+//
+// The arithmetic type T and the storage of the state come from the Policy (stage_f64.cuh:
+// plain FP64; stage_mixed.cuh: FP32 arithmetic on a compensated hi/lo FP32 state).
+#pragma once
+
+#include "physics.cuh"
+#include "runtime_types.cuh"
+
+namespace mhdb {
+
+template <int TX, int TY>
+struct TileShape {
+    static constexpr int HX = TX + 4;
+    static constexpr int HY = TY + 4;
+    static constexpr int NH = HX * HY;          // halo cells
+    static constexpr int SXN = TY * (TX + 2);   // x-sweep face-state cells
+    static constexpr int SYN = (TY + 2) * TX;   // y-sweep face-state cells
+    static constexpr int SN = SXN > SYN ? SXN : SYN;
+    static constexpr int NFX = (TX + 1) * TY;   // x-faces
+    static constexpr int NFY = TX * (TY + 1);   // y-faces
+    static constexpr int NF = NFX > NFY ? NFX : NFY;
+    static constexpr int JX = TX + 2;
+    static constexpr int JY = TY + 2;
+    static constexpr int NJ = JX * JY;          // current cells
+    static constexpr int NC = TX * TY;          // owned cells
+};
+
+template <class T, int TX, int TY, bool NI>
+constexpr size_t stage_smem_bytes()
+{
+    using S = TileShape<TX, TY>;
+    return sizeof(T) * (9 * S::NH + 9 * S::SN + 9 * S::NF + (NI ? 3 * S::NJ : 0));
+}
+
+// Slope sweep: for each cell of the sweep region and each component, the limited slope
+// s = lim(W - W_prev, W_next - W) (include/mhd/kernels/muscl_hll.hpp:64-65).
+template <int L, class T, int TX, int TY, int NT, bool YDIR>
+__device__ __forceinline__ void face_states(const T* __restrict__ sW, T* __restrict__ sS)
+{
+    using S = TileShape<TX, TY>;
+    constexpr int HX = S::HX;
+    constexpr int W = YDIR ? TX : TX + 2;       // sweep region width
+    constexpr int N = YDIR ? S::SYN : S::SXN;
+    constexpr int step = YDIR ? HX : 1;
+    for (int t = threadIdx.x; t < N; t += NT) {
+        const int sx = t % W, sy = t / W;
+        // halo coordinates of the cell (x: columns 1..TX+2, rows 2..TY+1; y: cols 2..TX+1,
+        // rows 1..TY+2)
+        const int i = YDIR ? (sy + 1) * HX + (sx + 2) : (sy + 2) * HX + (sx + 1);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const T* w = sW + c * S::NH + i;
+            const T wm = w[-step], w0 = w[0], wp = w[step];
+            sS[c * S::SN + t] = limit_slope<L>(w0 - wm, wp - w0);
+        }
+    }
+}
+
+// One face flux from the slopes and centre values of its two cells: left state W(l) + s(l)/2,
+// right state W(r) - s(r)/2 (include/mhd/kernels/muscl_hll.hpp:66-67), with the both-sides
+// first-order fallback of muscl_hll.hpp:145-168. Output in physical component order.
+template <class T>
+__device__ __forceinline__ void face_flux(const T* __restrict__ sS, int sn, int il, int ir,
+                                          const T* __restrict__ sW, int nh, int wl, int wr,
+                                          bool ydir, T gamma, T inv_gm1, T c_h, T* out)
+{
+    // physical component feeding each rotated-frame slot (rho, vn, vt, vz, p, bn, bt, bz, psi)
+    int comp[9] = {0, ydir ? 2 : 1, ydir ? 1 : 2, 3, 4, ydir ? 6 : 5, ydir ? 5 : 6, 7, 8};
+    T l[9], r[9], lc[9], rc[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int c = comp[q];
+        lc[q] = sW[c * nh + wl];
+        rc[q] = sW[c * nh + wr];
+        l[q] = lc[q] + T(0.5) * sS[c * sn + il];
+        r[q] = rc[q] - T(0.5) * sS[c * sn + ir];
+    }
+    const T inf = T(INFINITY);
+    const bool ok = (l[0] > T(0)) && (l[4] > T(0)) && (l[0] < inf) && (l[4] < inf) &&
+                    (r[0] > T(0)) && (r[4] > T(0)) && (r[0] < inf) && (r[4] < inf);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        l[q] = ok ? l[q] : lc[q];
+        r[q] = ok ? r[q] : rc[q];
+    }
+    const PrimN<T> WL{l[0], l[1], l[2], l[3], l[4], l[5], l[6], l[7], l[8]};
+    const PrimN<T> WR{r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]};
+    const FluxN<T> f = hll_flux(WL, WR, gamma, inv_gm1, c_h);
+    out[0] = f.rho;
+    out[1] = ydir ? f.mt : f.mn;
+    out[2] = ydir ? f.mn : f.mt;
+    out[3] = f.mz;
+    out[4] = f.e;
+    out[5] = ydir ? f.bt : f.bn;
+    out[6] = ydir ? f.bn : f.bt;
+    out[7] = f.bz;
+    out[8] = f.psi;
+}
+
+// Fluxes of all faces of one sweep into sF, then each owned cell's flux difference into dF.
+template <class T, int TX, int TY, int NT, bool YDIR, bool NI>
+__device__ __forceinline__ void face_sweep(const T* __restrict__ sW, const T* __restrict__ sS,
+                                           T* __restrict__ sF, const T* __restrict__ sJ,
+                                           const NonIdealCoef& ni, T gamma, T inv_gm1, T c_h,
+                                           T (&dF)[(TX * TY + NT - 1) / NT][9])
+{
+    using S = TileShape<TX, TY>;
+    constexpr int HX = S::HX;
+    constexpr int NFACE = YDIR ? S::NFY : S::NFX;
+    constexpr int FW = YDIR ? TX : TX + 1;      // faces per row
+    constexpr int SW = YDIR ? TX : TX + 2;      // face-state region width
+    for (int t = threadIdx.x; t < NFACE; t += NT) {
+        const int fx = t % FW, fy = t / FW;
+        // cells left/below (l) and right/above (r) of the face in face-state coordinates
+        const int ir = YDIR ? (fy + 1) * SW + fx : fy * SW + (fx + 1);
+        const int il = YDIR ? fy * SW + fx : fy * SW + fx;
+        // the same two cells in halo coordinates
+        const int wr = (fy + 2) * HX + (fx + 2);
+        const int wl = wr - (YDIR ? HX : 1);
+        T out[9];
+        face_flux(sS, S::SN, il, ir, sW, S::NH, wl, wr, YDIR, gamma, inv_gm1, c_h, out);
+        if constexpr (NI) {
+            // Face-averaged J and B, E from Ohm's law (include/mhd/rhs.hpp:75-114).
+            const int jr = (fy + 1) * S::JX + (fx + 1);
+            const int jl = jr - (YDIR ? S::JX : 1);
+            const T Jx = T(0.5) * (sJ[jl] + sJ[jr]);
+            const T Jy = T(0.5) * (sJ[S::NJ + jl] + sJ[S::NJ + jr]);
+            const T Jz = T(0.5) * (sJ[2 * S::NJ + jl] + sJ[2 * S::NJ + jr]);
+            const T Bx = T(0.5) * (sW[5 * S::NH + wl] + sW[5 * S::NH + wr]);
+            const T By = T(0.5) * (sW[6 * S::NH + wl] + sW[6 * S::NH + wr]);
+            const T Bz = T(0.5) * (sW[7 * S::NH + wl] + sW[7 * S::NH + wr]);
+            T Ex, Ey, Ez;
+            nonideal_e(Jx, Jy, Jz, Bx, By, Bz, ni, Ex, Ey, Ez);
+            if (!YDIR) {
+                out[6] += -Ez;
+                out[7] += Ey;
+                out[4] += By * Ez - Bz * Ey;
+            } else {
+                out[5] += Ez;
+                out[7] += -Ex;
+                out[4] += Bz * Ex - Bx * Ez;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            sF[c * S::NF + t] = out[c];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < (TX * TY + NT - 1) / NT; ++r) {
+        const int t = threadIdx.x + r * NT;
+        if (t < S::NC) {
+            const int cx = t % TX, cy = t / TX;
+            const int f0 = YDIR ? cy * TX + cx : cy * (TX + 1) + cx;
+            const int f1 = f0 + (YDIR ? TX : 1);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                dF[r][c] = sF[c * S::NF + f1] - sF[c * S::NF + f0];
+            }
+        }
+    }
+}
+
+template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::Args a)
+{
+    using T = typename Policy::T;
+    using S = TileShape<TX, TY>;
+    constexpr int HX = S::HX;
+    constexpr int R = (TX * TY + NT - 1) / NT; // owned cells per thread
+    const Ctrl* __restrict__ ctrl = a.ctrl;
+    if (ctrl->finished != 0) {
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sW = reinterpret_cast<T*>(smem_raw); // [9][HY][HX] primitives
+    T* sS = sW + 9 * S::NH;                 // [9][SN] limited slopes of the current sweep
+    T* sF = sS + 9 * S::SN;                 // [9][NF] face fluxes
+    T* sJ = sF + 9 * S::NF;                 // [3][JY][JX] current
+
+    const Geometry& g = a.geom;
+    const Consts& k = a.k;
+    const int x0 = blockIdx.x * TX;
+    const int y0 = blockIdx.y * TY;
+    const double dt = ctrl->dt;
+    const double c_h64 = ctrl->c_h;
+    const T c_h = static_cast<T>(c_h64);
+    const T gamma = static_cast<T>(k.gamma);
+    const T inv_gm1 = static_cast<T>(k.inv_gm1);
+
+    // A. tile + halo as primitives
+    for (int t = threadIdx.x; t < S::NH; t += NT) {
+        const int lx = t % HX, ly = t / HX;
+        const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+        const int sx = map_index(gx, g.nx, g.bc_x);
+        const int sy = map_index(gy, g.ny, g.bc_y);
+        const bool interior = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
+        T w[9];
+        if (MASK && a.walls && interior && is_solid(a.mask, g, sx, sy)) {
+            double f[9];
+            Policy::wall_fill(a.uin, a.mask, g, sx, sy, k.gm1, f);
+            Policy::prim_of(f, k, w);
+        } else {
+            Policy::halo_prim(a.uin, g, sx, sy, k, w);
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            sW[c * S::NH + t] = w[c];
+        }
+    }
+    __syncthreads();
+
+    // B. current J (include/mhd/nonideal.hpp:30-60)
+    if constexpr (NI) {
+        const T inv_2dx = static_cast<T>(k.inv_2dx), inv_2dy = static_cast<T>(k.inv_2dy);
+        for (int t = threadIdx.x; t < S::NJ; t += NT) {
+            const int jx = t % S::JX + 1, jy = t / S::JX + 1;
+            const int i = jy * HX + jx;
+            const T* bx = sW + 5 * S::NH;
+            const T* by = sW + 6 * S::NH;
+            const T* bz = sW + 7 * S::NH;
+            const T dbz_dy = (bz[i + HX] - bz[i - HX]) * inv_2dy;
+            const T dbz_dx = (bz[i + 1] - bz[i - 1]) * inv_2dx;
+            const T dby_dx = (by[i + 1] - by[i - 1]) * inv_2dx;
+            const T dbx_dy = (bx[i + HX] - bx[i - HX]) * inv_2dy;
+            sJ[0 * S::NJ + t] = dbz_dy;
+            sJ[1 * S::NJ + t] = -dbz_dx;
+            sJ[2 * S::NJ + t] = dby_dx - dbx_dy;
+        }
+    }
+
+    // C. x sweep
+    T dFx[R][9];
+    face_states<L, T, TX, TY, NT, false>(sW, sS);
+    __syncthreads();
+    face_sweep<T, TX, TY, NT, false, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dFx);
+    __syncthreads();
+    // D. y sweep
+    T dGy[R][9];
+    face_states<L, T, TX, TY, NT, true>(sW, sS);
+    __syncthreads();
+    face_sweep<T, TX, TY, NT, true, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dGy);
+
+    // E. divergence, psi damping, solid zeroing and the stage update
+    const T inv_dx = static_cast<T>(k.inv_dx), inv_dy = static_cast<T>(k.inv_dy);
+    const double psi_damp = (c_h64 > 0.0 && k.glm_alpha > 0.0) ? (c_h64 * k.glm_alpha / k.h) : 0.0;
+    double smax = 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = threadIdx.x + r * NT;
+        if (t >= S::NC) {
+            continue;
+        }
+        const int cx = t % TX, cy = t / TX;
+        const int gx = x0 + cx, gy = y0 + cy;
+        if (gx >= g.nx || gy >= g.ny) {
+            continue;
+        }
+        const bool solid = MASK && is_solid(a.mask, g, gx, gy);
+        double Lc[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            // include/mhd/rhs.hpp:121
+            Lc[c] = static_cast<double>(-dFx[r][c] * inv_dx - dGy[r][c] * inv_dy);
+        }
+        double uin[9];
+        if (solid && a.walls) {
+            Policy::wall_fill(a.uin, a.mask, g, gx, gy, k.gm1, uin);
+        } else {
+            Policy::load_full(a.uin, g, gx, gy, uin);
+        }
+        if (psi_damp != 0.0) {
+            Lc[8] -= psi_damp * uin[8]; // include/mhd/rhs.hpp:219-225
+        }
+        if (solid) {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                Lc[c] = 0.0;
+            }
+        }
+        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        if constexpr (STAGE == 1) {
+            // include/mhd/field_ops.hpp:51: U* = U + dt L
+            double r1[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                r1[c] = uin[c] + dt * Lc[c];
+            }
+            Policy::store(a.out, g, o, r1);
+        } else {
+            // uin = U*, out = U^n updated in place (include/mhd/field_ops.hpp:61). For solid
+            // cells U*'s stored value is the (wall-filled) U^n written by stage 1.
+            double un[9];
+            if (solid) {
+                Policy::load_full(a.uin, g, gx, gy, un);
+            } else {
+                Policy::load_full(a.out, g, gx, gy, un);
+            }
+            const double half_dt = 0.5 * dt;
+            double r2[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                r2[c] = 0.5 * (un[c] + uin[c]) + half_dt * Lc[c];
+            }
+            Policy::store(a.out, g, o, r2);
+            if (!solid) {
+                smax = vmax(smax, Policy::signal_speed(r2, k));
+            }
+        }
+    }
+
+    if constexpr (STAGE == 2) {
+        reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
+    }
+}
+
+} // namespace mhdb

@@ -1,0 +1,40 @@
+// Host-side table of the compiled stage-kernel instantiations. Each precision form is compiled
+// in its own translation unit (kernels_f64.cu, kernels_mixed.cu) for a few tile configurations;
+// configuration 0 is the default and the only one instantiated for every combination of limiter,
+// non-ideal terms and mask. The other configurations exist for the ideal, unmasked case and are
+// chosen by the autotuner (mhdb_autotune) per grid size class.
+#pragma once
+
+#include <cstddef>
+
+#include "stage_f64.cuh"
+#include "stage_mixed.cuh"
+
+namespace mhdb {
+
+using StageFnF64 = void (*)(StageArgsF64);
+using StageFnMx = void (*)(StageArgsMx);
+
+struct StageKernels {
+    StageFnF64 f64_stage1 = nullptr, f64_stage2 = nullptr;
+    StageFnMx mx_stage1 = nullptr, mx_stage2 = nullptr;
+    int tile_x = 0, tile_y = 0, threads = 0;
+    size_t smem = 0; // 0: no such configuration
+};
+
+struct TileConfigInfo {
+    int tile_x, tile_y, threads, min_blocks;
+};
+
+// Number of tile configurations compiled per precision form, and their shapes.
+int stage_config_count_f64();
+int stage_config_count_mixed();
+TileConfigInfo stage_config_info_f64(int config);
+TileConfigInfo stage_config_info_mixed(int config);
+
+// Kernels of one configuration; config != 0 is available only for ideal, unmasked solves
+// (smem == 0 otherwise).
+StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
+StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);
+
+} // namespace mhdb

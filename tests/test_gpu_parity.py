@@ -276,3 +276,23 @@ def test_fp32_mixed_within_1e6_of_fp64_oracle(case):
     core = [0, 1, 2, 4, 5, 6]
     assert np.all(err[core] <= MIXED_L1), err
     print(case, "rel L1 FP32-mixed vs FP64 oracle:", err)
+
+
+@pytest.mark.parametrize("precision", [_capi.FP64, _capi.FP32])
+def test_every_tile_configuration_matches_oracle(precision):
+    nx, ny = 70, 45
+    U0 = initial_state(wl.fourier_state(nx, ny, 4), 5.0 / 3.0)
+    p = orc.Params(limiter=orc.VANLEER, max_steps=20, fixed_steps=True)
+    ref, tr, sr, _ = orc.solve(U0, orc.Grid(nx, ny), p)
+    tol = FP64_L1 if precision == _capi.FP64 else MIXED_L1
+    for cfg in _capi.tile_configs(precision):
+        dev = _capi.DeviceSolver(nx, ny, precision=precision)
+        dev.set_tile_config(cfg["config"])
+        dev.configure(0, 0)
+        dev.upload(U0)
+        r = dev.solve_steps(_capi.make_params(limiter=_capi.VANLEER), 20)
+        got = dev.download()
+        dev.close()
+        assert r.steps == sr
+        err = rel_l1(got, ref)
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (cfg, err)

@@ -1,0 +1,127 @@
+"""Host-side logic without a GPU: the numpy ghost fill and wall fill of the Python surface
+against the oracle, the boundary index maps, and the seeded workload generators."""
+
+import numpy as np
+import pytest
+
+from mhd_gpu_solver_b200 import mhd_solver as ms
+from mhd_gpu_solver_b200 import workloads as wl
+from oracle import oracle as orc
+
+
+@pytest.mark.parametrize("nx,ny", [(1, 1), (1, 3), (3, 1), (2, 5), (7, 4), (33, 9)])
+@pytest.mark.parametrize("bc", [(0, 0), (2, 2), (0, 2), (2, 0)])
+@pytest.mark.parametrize("ng", [2, 3])
+def test_ghost_fill_matches_reference_order(nx, ny, bc, ng):
+    rng = np.random.Generator(np.random.PCG64(nx * 100 + ny))
+    U = rng.standard_normal((9, ny + 2 * ng, nx + 2 * ng))
+    ref = orc.apply_bc(U, orc.Grid(nx, ny, ng), bc)
+    got = U.copy()
+    ms.apply_boundary_conditions(got, nx, ny, ng, bc[0], bc[1])
+    assert np.array_equal(got, ref)
+
+
+def test_reflective_boundary_is_rejected():
+    U = np.zeros((9, 8, 8))
+    with pytest.raises(ValueError, match="Reflective"):
+        ms.apply_boundary_conditions(U, 4, 4, 2, 1, 0)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_wall_fill_bitwise_equal_to_oracle(seed):
+    nx, ny = 29, 23
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mask = (rng.uniform(size=(ny, nx)) > 0.3).astype(np.uint8)
+    mask[5:9, 5:9] = 0  # an interior solid block with cells that have no fluid neighbour
+    prim = wl.fourier_state(nx, ny, seed)
+    U = wl.embed(wl.to_conservative(prim, 1.4))
+    U = orc.apply_bc(U, orc.Grid(nx, ny), (0, 2))
+    ref = orc.wall_fill(U, orc.Grid(nx, ny), mask, 1.4)
+    got = U.copy()
+    ms.apply_solid_wall_fill(got, mask, 2, 1.4)
+    assert np.array_equal(got, ref)
+
+
+def test_workloads_are_seeded_and_shaped():
+    a = wl.fourier_state(64, 48, 3)
+    b = wl.fourier_state(64, 48, 3)
+    c = wl.fourier_state(64, 48, 4)
+    for k in wl.FIELDS:
+        assert a[k].shape == (48, 64)
+        assert np.array_equal(a[k], b[k])
+    assert not np.array_equal(a["vx"], c["vx"])
+    # velocity and field normalised to rms 1, perturbations clipped to [-0.2, 0.2]
+    assert abs(np.sqrt(np.mean(a["vx"] ** 2 + a["vy"] ** 2)) - 1.0) < 1e-12
+    assert abs(np.sqrt(np.mean(a["bx"] ** 2 + a["by"] ** 2)) - 1.0) < 1e-12
+    assert a["rho"].min() >= 0.8 - 1e-15 and a["rho"].max() <= 1.2 + 1e-15
+    assert a["p"].min() >= 0.8 - 1e-15 and a["p"].max() <= 1.2 + 1e-15
+    assert np.all(a["vz"] == 0) and np.all(a["bz"] == 0) and np.all(a["psi"] == 0)
+
+
+def test_fourier_field_is_divergence_free_in_the_continuum():
+    # Analytic curl of A_z: the spectral divergence of (bx, by) vanishes to round-off.
+    n = 64
+    f = wl.fourier_state(n, n, 1)
+    kx = np.fft.fftfreq(n) * n
+    BX, BY = np.fft.fft2(f["bx"]), np.fft.fft2(f["by"])
+    div = kx[None, :] * BX + kx[:, None] * BY
+    assert np.max(np.abs(div)) < 1e-9 * np.max(np.abs(BX))
+
+
+def test_quadrants_and_mask_generators():
+    q = wl.four_quadrant(16, 16, 0)
+    assert np.all(q["bx"] == 0.75)
+    assert len(np.unique(q["rho"])) == 4
+    assert q["rho"].min() >= 0.1 and q["rho"].max() <= 2.0
+    m = wl.circles_and_rectangles(256, 256, 0)
+    assert m.dtype == np.uint8 and set(np.unique(m)) <= {0, 1}
+    assert 0.01 < 1.0 - m.mean() < 0.6
+    assert np.array_equal(m, wl.circles_and_rectangles(256, 256, 0))
+
+
+def test_python_surface_names_match_reference_module():
+    names = ["set_num_threads", "num_threads", "set_simd_enabled", "simd_enabled",
+             "simd_backend", "simd_width", "metal_available", "cuda_available",
+             "available_backends", "SlopeLimiter", "BoundaryConditionType", "NonIdealConfig",
+             "SolveResult", "SolveParams", "MHDSolver"]
+    for n in names:
+        assert hasattr(ms, n), n
+    methods = ["set_periodic_bc", "set_outflow_bc", "set_bc", "set_gamma", "set_cfl",
+               "set_glm_alpha", "set_limiter_minmod", "set_limiter_mc", "set_ideal",
+               "enable_ohmic", "enable_hall", "enable_ambipolar", "disable_ohmic",
+               "disable_hall", "disable_ambipolar", "set_mask", "get_mask", "clear_mask",
+               "set_walls_reflective", "walls_reflective", "set_field", "set_primitives",
+               "initialize", "set_backend", "backend", "backend_device", "run", "advance_to",
+               "time", "steps", "c_h", "max_div_b", "field", "nx", "ny", "ng", "size_x",
+               "size_y", "x_min", "x_max", "y_min", "y_max", "params"]
+    for n in methods:
+        assert hasattr(ms.MHDSolver, n), n
+    p = ms.SolveParams()
+    assert (p.t_end, p.cfl, p.gamma, p.glm_alpha, p.limiter, p.max_steps) == (
+        0.0, 0.4, 5.0 / 3.0, 0.1, ms.SlopeLimiter.MC, 1_000_000)
+    ni = ms.NonIdealConfig.with_ohmic(0.0)
+    assert not ni.any()
+    assert ni.enable_hall(1e-2).any()
+
+
+def test_host_state_preparation_without_device():
+    s = ms.MHDSolver(16, 12)
+    s.set_outflow_bc()
+    s.initialize("orszag_tang")
+    rho = s.field("rho")
+    assert rho.shape == (16, 20)
+    assert np.all(rho[0] == rho[2]) and np.all(rho[:, 0] == rho[:, 2])
+    m = np.ones((12, 16), np.uint8)
+    m[4:6, 4:8] = 0
+    s.set_mask(m)
+    assert np.array_equal(s.get_mask(), m)
+    with pytest.raises(ValueError):
+        s.set_mask(np.ones((3, 3), np.uint8))
+    with pytest.raises(ValueError, match="Unknown field"):
+        s.field("nope")
+    with pytest.raises(ValueError, match="Unknown initial condition"):
+        s.initialize("nope")
+    with pytest.raises(RuntimeError, match="Backend not available: cpu"):
+        s.set_backend("cpu")
+    with pytest.raises(ValueError, match="Unknown backend"):
+        s.set_backend("tpu")
