@@ -143,6 +143,32 @@ int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, i
                           int* min_blocks);
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
+/* Allocation-free fixed-step solve. No counterpart in the reference.
+   For callers that cannot call cudaMalloc: code inside another framework's device memory pool or
+   under a fixed memory budget, and code that must not let an allocation synchronise the device.
+   Advances an FP64 state that the caller owns in device memory by exactly nsteps SSP-RK2 steps
+   (no t_end limit, like mhdb_solve_steps), without a handle and without allocating anything:
+   the stage state U* and the step control live in one file-scope device array of 16 MiB + 256 B
+   that every GPU loading this library holds until the process exits.
+   - u_in, u_out: device pointers to 9 dense planes of nx * ny doubles (rho, mx, my, mz, E, bx,
+     by, bz, psi; interior cells only, row-major, no ghosts); u_out may equal u_in. The caller
+     passes both; the state is read from u_in and the result written to u_out.
+   - Limit: nx * ny <= 233016 interior cells (16 MiB / 72 B); larger grids are rejected with
+     MHDB_INVALID_ARGUMENT and a message from mhdb_last_error(NULL). No mask; boundaries
+     periodic or outflow; ideal or non-ideal terms, any limiter.
+   - Work runs on `stream` (a cudaStream_t, NULL for the legacy default stream); the call returns
+     after the stream has finished the solve and result holds t, steps and c_h.
+   - The first call on each device looks up the device address of the scratch array
+     (cudaGetSymbolAddress) with that device current; make that first call before any stream
+     capture.
+   - Every call shares the one scratch array, which keeps the last call's contents: the step
+     control is reset at the start of each call and U* is fully rewritten before it is read.
+     Calls whose work overlaps on the GPU (several streams, threads or processes sharing the
+     library on one device) race on that array. */
+int mhdb_solve_steps_noalloc_f64(const mhdb_grid* grid, int bc_x, int bc_y,
+                                 const mhdb_params* params, int nsteps, const double* u_in,
+                                 double* u_out, mhdb_result* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

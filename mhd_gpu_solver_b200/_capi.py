@@ -26,7 +26,7 @@ EXPORTS = (
     "mhdb_precision", "mhdb_configure", "mhdb_upload", "mhdb_download", "mhdb_solve",
     "mhdb_solve_steps", "mhdb_diagnostics", "mhdb_stream", "mhdb_set_profiling",
     "mhdb_profile_read", "mhdb_launch_count", "mhdb_tile_config_count", "mhdb_tile_config_info",
-    "mhdb_set_tile_config",
+    "mhdb_set_tile_config", "mhdb_solve_steps_noalloc_f64",
 )
 
 
@@ -87,6 +87,9 @@ def _load() -> C.CDLL:
         "mhdb_tile_config_info": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "mhdb_set_tile_config": ([h, C.c_int], C.c_int),
+        "mhdb_solve_steps_noalloc_f64": ([C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(Params),
+                                          C.c_int, C.c_void_p, C.c_void_p, C.POINTER(Result),
+                                          C.c_void_p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -31,9 +31,12 @@
 
 using namespace mhdb;
 
-namespace {
-
+namespace mhdb {
+// Message of the last failure not tied to a handle (mhdb_last_error(NULL)).
 thread_local std::string g_create_error;
+} // namespace mhdb
+
+namespace {
 
 struct CudaFail {
     cudaError_t err;
