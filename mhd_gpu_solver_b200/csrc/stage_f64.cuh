@@ -69,40 +69,84 @@ struct StageArgsF64 {
 struct PolicyF64 {
     using T = double;
     using Args = StageArgsF64;
+    struct Raw {
+        double v[9];
+    };
 
-    static __device__ __forceinline__ void halo_prim(const double* u, const Geometry& g, int x,
-                                                     int y, const Consts& k, double* w)
+    static __device__ __forceinline__ void load_raw(const Args& a, const Geometry& g, int x, int y,
+                                                    Raw& r)
     {
-        double c[9];
-        load_cons_f64(u, g, x, y, c);
-        cons_to_prim(c, k.gm1, w);
+        load_cons_f64(a.uin, g, x, y, r.v);
+    }
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void raw_prim(const Args&, const Geometry&, int, int,
+                                                    const Raw& r, const Consts& k, double* w)
+    {
+        cons_to_prim(r.v, k.gm1, w);
     }
     static __device__ __forceinline__ void prim_of(const double* f, const Consts& k, double* w)
     {
         cons_to_prim(f, k.gm1, w);
     }
-    static __device__ __forceinline__ void wall_fill(const double* u, const uint8_t* mask,
-                                                     const Geometry& g, int x, int y, double gm1,
-                                                     double* out)
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void wall_fill(const Args& a, const Geometry& g, int x,
+                                                     int y, double gm1, double* out)
     {
-        wall_fill_f64(u, mask, g, x, y, gm1, out);
-    }
-    static __device__ __forceinline__ void load_full(const double* u, const Geometry& g, int x,
-                                                     int y, double* out)
-    {
-        load_cons_f64(u, g, x, y, out);
-    }
-    static __device__ __forceinline__ void store(double* u, const Geometry& g, size_t o,
-                                                 const double* v)
-    {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            u[static_cast<size_t>(c) * g.plane + o] = v[c];
-        }
+        wall_fill_f64(a.uin, a.mask, g, x, y, gm1, out);
     }
     static __device__ __forceinline__ double signal_speed(const double* r, const Consts& k)
     {
         return cell_max_signal_speed(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], k.gamma);
+    }
+
+    // Stage update of one owned cell: stage 1 U* = U + dt L (include/mhd/field_ops.hpp:51);
+    // stage 2 U = (U + U*)/2 + (dt/2) L in place (field_ops.hpp:61). For a solid cell the stored
+    // U* is the (wall-filled) U^n written by stage 1 and the stage input is the fill of U*.
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void update(const Args& a, const Geometry& g, int gx, int gy,
+                                                  bool solid, double (&L)[9], double psi_in,
+                                                  double psi_damp, double dt, const Consts& k,
+                                                  double& smax)
+    {
+        if (psi_damp != 0.0) {
+            L[8] -= psi_damp * psi_in; // include/mhd/rhs.hpp:219-225
+        }
+        if (solid) {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                L[c] = 0.0;
+            }
+        }
+        double uin[9];
+        if (solid && a.walls) {
+            wall_fill_f64(a.uin, a.mask, g, gx, gy, k.gm1, uin);
+        } else {
+            load_cons_f64(a.uin, g, gx, gy, uin);
+        }
+        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        if constexpr (STAGE == 1) {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                a.out[static_cast<size_t>(c) * g.plane + o] = uin[c] + dt * L[c];
+            }
+        } else {
+            double un[9];
+            if (solid) {
+                load_cons_f64(a.uin, g, gx, gy, un);
+            } else {
+                load_cons_f64(a.out, g, gx, gy, un);
+            }
+            const double half_dt = 0.5 * dt;
+            double r2[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                r2[c] = 0.5 * (un[c] + uin[c]) + half_dt * L[c];
+                a.out[static_cast<size_t>(c) * g.plane + o] = r2[c];
+            }
+            if (!solid) {
+                smax = vmax(smax, signal_speed(r2, k));
+            }
+        }
     }
 };
 

@@ -184,18 +184,17 @@ __device__ __forceinline__ void face_sweep(const T* __restrict__ sW, const T* __
     }
 }
 
-template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::Args a)
+// Phases A-E for the tile with lower-left interior cell (x0, y0); returns the largest signal
+// speed of the owned fluid cells after a stage-2 update (0 for stage 1).
+template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT>
+__device__ __forceinline__ double stage_tile(const typename Policy::Args& a, int x0, int y0,
+                                             unsigned char* smem_raw)
 {
     using T = typename Policy::T;
     using S = TileShape<TX, TY>;
     constexpr int HX = S::HX;
     constexpr int R = (TX * TY + NT - 1) / NT; // owned cells per thread
     const Ctrl* __restrict__ ctrl = a.ctrl;
-    if (ctrl->finished != 0) {
-        return;
-    }
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sW = reinterpret_cast<T*>(smem_raw); // [9][HY][HX] primitives
     T* sS = sW + 9 * S::NH;                 // [9][SN] limited slopes of the current sweep
     T* sF = sS + 9 * S::SN;                 // [9][NF] face fluxes
@@ -203,32 +202,54 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::
 
     const Geometry& g = a.geom;
     const Consts& k = a.k;
-    const int x0 = blockIdx.x * TX;
-    const int y0 = blockIdx.y * TY;
     const double dt = ctrl->dt;
     const double c_h64 = ctrl->c_h;
     const T c_h = static_cast<T>(c_h64);
     const T gamma = static_cast<T>(k.gamma);
     const T inv_gm1 = static_cast<T>(k.inv_gm1);
 
-    // A. tile + halo as primitives
-    for (int t = threadIdx.x; t < S::NH; t += NT) {
-        const int lx = t % HX, ly = t / HX;
-        const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-        const int sx = map_index(gx, g.nx, g.bc_x);
-        const int sy = map_index(gy, g.ny, g.bc_y);
-        const bool interior = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
-        T w[9];
-        if (MASK && a.walls && interior && is_solid(a.mask, g, sx, sy)) {
-            double f[9];
-            Policy::wall_fill(a.uin, a.mask, g, sx, sy, k.gm1, f);
-            Policy::prim_of(f, k, w);
-        } else {
-            Policy::halo_prim(a.uin, g, sx, sy, k, w);
+    // A. tile + halo as primitives. All loads of a thread are issued before any conversion so
+    // that they are in flight together.
+    {
+        constexpr int HR = (S::NH + NT - 1) / NT;
+        typename Policy::Raw raw[HR];
+        int src[HR][2];
+        bool fill[HR];
+#pragma unroll
+        for (int r = 0; r < HR; ++r) {
+            const int t = threadIdx.x + r * NT;
+            fill[r] = false;
+            if (t < S::NH) {
+                const int lx = t % HX, ly = t / HX;
+                const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+                const int sx = map_index(gx, g.nx, g.bc_x);
+                const int sy = map_index(gy, g.ny, g.bc_y);
+                const bool interior = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny;
+                src[r][0] = sx;
+                src[r][1] = sy;
+                fill[r] = MASK && a.walls && interior && is_solid(a.mask, g, sx, sy);
+                if (!fill[r]) {
+                    Policy::load_raw(a, g, sx, sy, raw[r]);
+                }
+            }
         }
 #pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            sW[c * S::NH + t] = w[c];
+        for (int r = 0; r < HR; ++r) {
+            const int t = threadIdx.x + r * NT;
+            if (t < S::NH) {
+                T w[9];
+                if (fill[r]) {
+                    double f[9];
+                    Policy::template wall_fill<STAGE, MASK>(a, g, src[r][0], src[r][1], k.gm1, f);
+                    Policy::prim_of(f, k, w);
+                } else {
+                    Policy::template raw_prim<STAGE, MASK>(a, g, src[r][0], src[r][1], raw[r], k, w);
+                }
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    sW[c * S::NH + t] = w[c];
+                }
+            }
         }
     }
     __syncthreads();
@@ -280,60 +301,79 @@ __global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::
             continue;
         }
         const bool solid = MASK && is_solid(a.mask, g, gx, gy);
-        double Lc[9];
+        T Lc[9];
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
-            // include/mhd/rhs.hpp:121
-            Lc[c] = static_cast<double>(-dFx[r][c] * inv_dx - dGy[r][c] * inv_dy);
+            Lc[c] = -dFx[r][c] * inv_dx - dGy[r][c] * inv_dy; // include/mhd/rhs.hpp:121
         }
-        double uin[9];
-        if (solid && a.walls) {
-            Policy::wall_fill(a.uin, a.mask, g, gx, gy, k.gm1, uin);
-        } else {
-            Policy::load_full(a.uin, g, gx, gy, uin);
-        }
-        if (psi_damp != 0.0) {
-            Lc[8] -= psi_damp * uin[8]; // include/mhd/rhs.hpp:219-225
-        }
-        if (solid) {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                Lc[c] = 0.0;
-            }
-        }
-        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
-        if constexpr (STAGE == 1) {
-            // include/mhd/field_ops.hpp:51: U* = U + dt L
-            double r1[9];
-#pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                r1[c] = uin[c] + dt * Lc[c];
-            }
-            Policy::store(a.out, g, o, r1);
-        } else {
-            // uin = U*, out = U^n updated in place (include/mhd/field_ops.hpp:61). For solid
-            // cells U*'s stored value is the (wall-filled) U^n written by stage 1.
-            double un[9];
-            if (solid) {
-                Policy::load_full(a.uin, g, gx, gy, un);
-            } else {
-                Policy::load_full(a.out, g, gx, gy, un);
-            }
-            const double half_dt = 0.5 * dt;
-            double r2[9];
-#pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                r2[c] = 0.5 * (un[c] + uin[c]) + half_dt * Lc[c];
-            }
-            Policy::store(a.out, g, o, r2);
-            if (!solid) {
-                smax = vmax(smax, Policy::signal_speed(r2, k));
-            }
-        }
+        const T psi_in = sW[8 * S::NH + (cy + 2) * HX + (cx + 2)];
+        Policy::template update<STAGE, MASK>(a, g, gx, gy, solid, Lc, psi_in, psi_damp, dt, k,
+                                             smax);
     }
+    return smax;
+}
 
+// One CTA per tile of one grid.
+template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::Args a)
+{
+    if (a.ctrl->finished != 0) {
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const double smax = stage_tile<Policy, L, NI, MASK, STAGE, TX, TY, NT>(
+        a, blockIdx.x * TX, blockIdx.y * TY, smem_raw);
     if constexpr (STAGE == 2) {
         reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
+    }
+}
+
+// One solve of a batch: its stage arguments and its tiling.
+template <class Policy>
+struct BatchSolve {
+    typename Policy::Args stage[2]; // stage 1 and stage 2 arguments
+    int tiles_x;                    // tiles per row
+    int ntiles;                     // tiles of this solve
+};
+
+// Persistent form over a tile work-list of many independent solves (each item: solve index,
+// tile index). Every CTA walks the list with a grid stride; a solve's signal-speed reduction
+// completes when its last tile arrives, whichever CTA processes it, and that tile advances the
+// solve's own FP64 clock. Finished solves are skipped.
+template <class Policy, int L, bool NI, int STAGE, int TX, int TY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) batch_stage_kernel(const BatchSolve<Policy>* solves,
+                                                              const int2* __restrict__ work,
+                                                              int nwork)
+{
+    using Args = typename Policy::Args;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) Args sa;
+    __shared__ int s_tiles_x, s_ntiles;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 it = work[w];
+        __syncthreads(); // the previous tile is done with shared memory
+        {
+            const int* src = reinterpret_cast<const int*>(&solves[it.x].stage[STAGE - 1]);
+            int* dst = reinterpret_cast<int*>(&sa);
+            for (int i = threadIdx.x; i < static_cast<int>(sizeof(Args) / sizeof(int)); i += NT) {
+                dst[i] = src[i];
+            }
+            if (threadIdx.x == 0) {
+                s_tiles_x = solves[it.x].tiles_x;
+                s_ntiles = solves[it.x].ntiles;
+            }
+        }
+        __syncthreads();
+        if (sa.ctrl->finished != 0) {
+            continue;
+        }
+        const int x0 = (it.y % s_tiles_x) * TX;
+        const int y0 = (it.y / s_tiles_x) * TY;
+        const double smax = stage_tile<Policy, L, NI, false, STAGE, TX, TY, NT>(sa, x0, y0, smem_raw);
+        if constexpr (STAGE == 2) {
+            reduce_signal_speed_and_finish(smax, sa.ctrl, sa.k, static_cast<unsigned>(s_ntiles),
+                                           true);
+        }
     }
 }
 

@@ -1,8 +1,10 @@
 // FP32-mixed form: the state is carried as a compensated pair of FP32 planes, value = hi + lo
 // with |lo| <= ulp(hi)/2 (~48 significant bits). Precision rules:
 //   * reconstruction, HLL fluxes, non-ideal terms and the divergence run in FP32 on hi;
-//   * the stage update is done in FP64 on hi + lo and split again, so the RK2 combination
-//     loses no bits;
+//   * the stage updates U* = U^n + dt L (include/mhd/field_ops.hpp:51) and
+//     U^{n+1} = (U^n + U*)/2 + (dt/2) L (field_ops.hpp:61) are done in double-FP32 arithmetic on
+//     the (hi, lo) pairs with error-free two-sums, so the RK2 combination loses no bits of the
+//     state (only the FP32 increment dt L carries FP32 rounding);
 //   * pressure recovery p = (gamma-1)(E - rho v^2/2 - B^2/2) is redone in FP64 from hi + lo in
 //     cells where the FP32 subtraction cancels (p/(gamma-1) < E / kCancelRatio: low beta or high
 //     Mach) or is not finite;
@@ -85,23 +87,54 @@ __device__ __forceinline__ bool cancels(const float* w, const float* uf, const C
     return !(eint * kCancelRatio >= uf[4]);
 }
 
+// Error-free transformation a + b = s + e (Knuth's two-sum; six FP32 additions, none of them
+// contractible).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e)
+{
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// Renormalise s + t (|t| small against s) into a (hi, lo) pair (Dekker's fast two-sum).
+__device__ __forceinline__ void fast_two_sum(float s, float t, float& h, float& l)
+{
+    h = s + t;
+    l = t - (h - s);
+}
+
 struct PolicyMixed {
     using T = float;
     using Args = StageArgsMx;
+    struct Raw {
+        float v[9];
+    };
 
-    static __device__ __forceinline__ void halo_prim(const MixedState& u, const Geometry& g,
-                                                     int x, int y, const Consts& k, float* w)
+    // Full-precision value of the stage input at (x, y): hi + lo.
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void full(const Args& a, const Geometry& g, int x, int y,
+                                                double* out)
+    {
+        load_cons_mx(a.uin, g, x, y, out);
+    }
+
+    static __device__ __forceinline__ void load_raw(const Args& a, const Geometry& g, int x, int y,
+                                                    Raw& r)
     {
         const size_t o = static_cast<size_t>(y) * g.pitch + x;
-        float uf[9];
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
-            uf[c] = __ldg(u.hi + static_cast<size_t>(c) * g.plane + o);
+            r.v[c] = __ldg(a.uin.hi + static_cast<size_t>(c) * g.plane + o);
         }
-        cons_to_prim(uf, static_cast<float>(k.gm1), w);
-        if (cancels(w, uf, k)) {
+    }
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void raw_prim(const Args& a, const Geometry& g, int x, int y,
+                                                    const Raw& r, const Consts& k, float* w)
+    {
+        cons_to_prim(r.v, static_cast<float>(k.gm1), w);
+        if (cancels(w, r.v, k)) {
             double d[9];
-            load_cons_mx(u, g, x, y, d);
+            full<STAGE, MASK>(a, g, x, y, d);
             w[4] = pressure_f64(d, k.gm1);
         }
     }
@@ -117,24 +150,17 @@ struct PolicyMixed {
             w[4] = pressure_f64(f, k.gm1);
         }
     }
-    static __device__ __forceinline__ void wall_fill(const MixedState& u, const uint8_t* mask,
-                                                     const Geometry& g, int x, int y, double gm1,
-                                                     double* out)
+    // FP64 wall fill of a solid cell from its fluid neighbours' full-precision stage input.
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void wall_fill(const Args& a, const Geometry& g, int x,
+                                                     int y, double gm1, double* out)
     {
-        wall_fill_mx(u, mask, g, x, y, gm1, out);
+        wall_fill_mx(a.uin, a.mask, g, x, y, gm1, out);
     }
-    static __device__ __forceinline__ void load_full(const MixedState& u, const Geometry& g,
-                                                     int x, int y, double* out)
+    static __device__ __forceinline__ float signal_speed_f(const float* r, const Consts& k)
     {
-        load_cons_mx(u, g, x, y, out);
-    }
-    static __device__ __forceinline__ void store(const MixedState& u, const Geometry& g, size_t o,
-                                                 const double* v)
-    {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            split_store(u, static_cast<size_t>(c) * g.plane + o, v[c]);
-        }
+        return cell_max_signal_speed(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7],
+                                     static_cast<float>(k.gamma));
     }
     static __device__ __forceinline__ double signal_speed(const double* r, const Consts& k)
     {
@@ -143,9 +169,95 @@ struct PolicyMixed {
         for (int c = 0; c < 8; ++c) {
             rf[c] = __double2float_rn(r[c]);
         }
-        return static_cast<double>(cell_max_signal_speed(rf[0], rf[1], rf[2], rf[3], rf[4], rf[5],
-                                                         rf[6], rf[7],
-                                                         static_cast<float>(k.gamma)));
+        return static_cast<double>(signal_speed_f(rf, k));
+    }
+
+    template <int STAGE, bool MASK>
+    static __device__ __forceinline__ void update(const Args& a, const Geometry& g, int gx, int gy,
+                                                  bool solid, float (&L)[9], float psi_in,
+                                                  double psi_damp, double dt, const Consts& k,
+                                                  double& smax)
+    {
+        if (psi_damp != 0.0) {
+            L[8] -= static_cast<float>(psi_damp) * psi_in; // include/mhd/rhs.hpp:219-225
+        }
+        if (solid) {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                L[c] = 0.0f;
+            }
+        }
+        const float dtf = static_cast<float>(dt);
+        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        if (MASK && solid && a.walls) {
+            // Rare path in FP64: stage 1 stores fill(U^n); stage 2 stores
+            // (U*_stored + fill(U*)) / 2, where the stored U* of a solid cell is fill(U^n).
+            double f[9];
+            wall_fill<STAGE, MASK>(a, g, gx, gy, k.gm1, f);
+            if constexpr (STAGE == 2) {
+                double un[9];
+                load_cons_mx(a.uin, g, gx, gy, un);
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    f[c] = 0.5 * (un[c] + f[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                split_store(a.out, static_cast<size_t>(c) * g.plane + o, f[c]);
+            }
+            return;
+        }
+        const float* __restrict__ ih = a.uin.hi;
+        const float* __restrict__ il = a.uin.lo;
+        float* __restrict__ oh = a.out.hi;
+        float* __restrict__ ol = a.out.lo;
+        // every load before any store
+        float xh[9], xl[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const size_t q = static_cast<size_t>(c) * g.plane + o;
+            xh[c] = __ldg(ih + q);
+            xl[c] = __ldg(il + q);
+        }
+        if constexpr (STAGE == 1) {
+            // U* = U^n + dt L
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                float s, e, h, l;
+                two_sum(xh[c], __fmul_rn(dtf, L[c]), s, e); // product rounded first: exact two-sum
+                fast_two_sum(s, xl[c] + e, h, l);
+                const size_t q = static_cast<size_t>(c) * g.plane + o;
+                oh[q] = h;
+                ol[q] = l;
+            }
+        } else {
+            // U^{n+1} = (U^n + U*)/2 + (dt/2) L, U^n read from the output buffer (own cell)
+            float nh[9], nl[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                const size_t q = static_cast<size_t>(c) * g.plane + o;
+                nh[c] = oh[q];
+                nl[c] = ol[q];
+            }
+            float rf[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                float s, e, h, l;
+                two_sum(nh[c], xh[c], s, e);
+                fast_two_sum(s, (nl[c] + xl[c]) + e, h, l);
+                // halving is exact; then add the increment
+                two_sum(0.5f * h, __fmul_rn(0.5f * dtf, L[c]), s, e);
+                fast_two_sum(s, 0.5f * l + e, h, l);
+                const size_t q = static_cast<size_t>(c) * g.plane + o;
+                oh[q] = h;
+                ol[q] = l;
+                rf[c] = h;
+            }
+            if (!solid) {
+                smax = vmax(smax, static_cast<double>(signal_speed_f(rf, k)));
+            }
+        }
     }
 };
 
