@@ -79,6 +79,22 @@ typedef struct {
 
 typedef struct mhdb_solver mhdb_solver;
 
+/* Seeded synthetic initial state generated on the device (additive): a smooth periodic field of
+   Fourier modes, or four piecewise-constant quadrants split at x = y = 0.5. For the Fourier kind,
+   coef holds 5 spectra (vx, vy, A_z, f1, f2), each (2 kmax + 1) rows (ky = -kmax..kmax) by
+   (kmax + 1) columns (kx = 0..kmax) of complex values as (re, im) pairs; the device evaluates them
+   at cell centres, sets B = curl(A_z), scales v and B to rms 1, and sets rho = 1 + clip(0.2 f1),
+   p = 1 + clip(0.1 f2) with f1, f2 scaled to rms 1 and the perturbations clipped to +-0.2. For
+   the quadrant kind, quad[q] = (rho, p, vx, vy, By) of quadrant q in the order (x<.5, y<.5),
+   (x>=.5, y<.5), (x<.5, y>=.5), (x>=.5, y>=.5), with Bx = 0.75. */
+enum { MHDB_INIT_FOURIER = 0, MHDB_INIT_QUADRANTS = 1 };
+typedef struct {
+    int kind;
+    int kmax;
+    const double* coef;
+    double quad[4][5];
+} mhdb_init;
+
 /* mhd::cuda_available() (device_solver.hpp:78): 1 when a CUDA device is usable. */
 int mhdb_cuda_available(void);
 
@@ -118,6 +134,11 @@ int mhdb_solve(mhdb_solver* h, const mhdb_params* params, mhdb_result* result);
 /* Additive: advance exactly nsteps SSP-RK2 steps (no t_end limit; params->t_end is ignored). */
 int mhdb_solve_steps(mhdb_solver* h, const mhdb_params* params, int nsteps, mhdb_result* result);
 
+/* Additive: replace the device state by a generated initial state (gamma from params). The
+   state then behaves like the result of a solve: download fills the ghosts, and with a mask the
+   next solve wall-fills the solid cells first. */
+int mhdb_generate(mhdb_solver* h, const mhdb_init* init, const mhdb_params* params);
+
 /* Additive: FP64 diagnostics of the device state (gamma from params). */
 int mhdb_diagnostics(mhdb_solver* h, const mhdb_params* params, mhdb_diag* out);
 
@@ -142,6 +163,41 @@ int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);
 int mhdb_set_tile_config(mhdb_solver* h, int config);
+
+/* ---------------------------------------------------------------- batched form (additive)
+
+   A batch advances many independent solves of uneven sizes together: every RK2 step is one
+   persistent launch per stage (per limiter and non-ideal combination present) over a tile
+   work-list of all unfinished solves, and chunks of steps are replayed as CUDA graphs. Each solve
+   has its own grid, physics parameters, boundary rule, time target and HBM-resident state, and
+   its own FP64 clock; results do not depend on what else is in the batch. No fluid masks. */
+typedef struct mhdb_batch mhdb_batch;
+
+int mhdb_batch_create(int precision, mhdb_batch** out);
+void mhdb_batch_destroy(mhdb_batch* b);
+const char* mhdb_batch_last_error(const mhdb_batch* b);
+
+/* Add a solve from a host state in the StateField layout (uploaded during the call). With
+   fixed_steps != 0 the solve runs exactly params->max_steps steps (t_end ignored); otherwise it
+   runs to params->t_end like mhdb_solve. *id identifies the solve until mhdb_batch_remove. */
+int mhdb_batch_add(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, int bc_x,
+                   int bc_y, const double* const comps[9], size_t n_tot, int fixed_steps,
+                   int* id);
+int mhdb_batch_remove(mhdb_batch* b, int id);
+
+/* Add a solve whose initial state is generated on the device (no host state, no upload). */
+int mhdb_batch_add_generated(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params,
+                             int bc_x, int bc_y, const mhdb_init* init, int fixed_steps, int* id);
+
+/* Advance every unfinished solve by up to nsteps steps; *active (optional) = unfinished count. */
+int mhdb_batch_step(mhdb_batch* b, int nsteps, int* active);
+
+/* t, steps, c_h and whether the solve has finished; MHDB_MAX_STEPS / MHDB_BAD_TIMESTEP as
+   mhdb_solve would report them. */
+int mhdb_batch_status(mhdb_batch* b, int id, mhdb_result* result, int* finished);
+int mhdb_batch_download(mhdb_batch* b, int id, double* const comps[9], size_t n_tot);
+int mhdb_batch_info(const mhdb_batch* b, size_t* bytes_in_use, int* live, long long* launches);
+void* mhdb_batch_stream(mhdb_batch* b);
 
 /* Allocation-free fixed-step solve. No counterpart in the reference.
    For callers that cannot call cudaMalloc: code inside another framework's device memory pool or

@@ -26,7 +26,10 @@ EXPORTS = (
     "mhdb_precision", "mhdb_configure", "mhdb_upload", "mhdb_download", "mhdb_solve",
     "mhdb_solve_steps", "mhdb_diagnostics", "mhdb_stream", "mhdb_set_profiling",
     "mhdb_profile_read", "mhdb_launch_count", "mhdb_tile_config_count", "mhdb_tile_config_info",
-    "mhdb_set_tile_config", "mhdb_solve_steps_noalloc_f64",
+    "mhdb_set_tile_config", "mhdb_solve_steps_noalloc_f64", "mhdb_batch_create",
+    "mhdb_batch_destroy", "mhdb_batch_last_error", "mhdb_batch_add", "mhdb_batch_remove",
+    "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download", "mhdb_batch_info",
+    "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
 )
 
 
@@ -52,6 +55,13 @@ class Diag(C.Structure):
                 ("div_b_l2", C.c_double), ("rho_min", C.c_double), ("p_min", C.c_double),
                 ("finite", C.c_int)]
 
+
+class Init(C.Structure):
+    _fields_ = [("kind", C.c_int), ("kmax", C.c_int), ("coef", C.POINTER(C.c_double)),
+                ("quad", (C.c_double * 5) * 4)]
+
+
+INIT_FOURIER, INIT_QUADRANTS = 0, 1
 
 _PD = C.POINTER(C.c_double)
 _PPD = C.POINTER(_PD)
@@ -91,6 +101,24 @@ def _load() -> C.CDLL:
                                           C.c_int, C.c_void_p, C.c_void_p, C.POINTER(Result),
                                           C.c_void_p], C.c_int),
     }
+    b = C.c_void_p
+    sig.update({
+        "mhdb_batch_create": ([C.c_int, C.POINTER(b)], C.c_int),
+        "mhdb_batch_destroy": ([b], None),
+        "mhdb_batch_last_error": ([b], C.c_char_p),
+        "mhdb_batch_add": ([b, C.POINTER(Grid), C.POINTER(Params), C.c_int, C.c_int, _PPD,
+                            C.c_size_t, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mhdb_batch_remove": ([b, C.c_int], C.c_int),
+        "mhdb_batch_step": ([b, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mhdb_batch_status": ([b, C.c_int, C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
+        "mhdb_batch_download": ([b, C.c_int, _PPD, C.c_size_t], C.c_int),
+        "mhdb_batch_info": ([b, C.POINTER(C.c_size_t), C.POINTER(C.c_int),
+                             C.POINTER(C.c_longlong)], C.c_int),
+        "mhdb_batch_stream": ([b], C.c_void_p),
+        "mhdb_batch_add_generated": ([b, C.POINTER(Grid), C.POINTER(Params), C.c_int, C.c_int,
+                                      C.POINTER(Init), C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mhdb_generate": ([h, C.POINTER(Init), C.POINTER(Params)], C.c_int),
+    })
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
         fn.argtypes = args
@@ -230,6 +258,11 @@ class DeviceSolver:
     def launch_count(self) -> int:
         return int(lib.mhdb_launch_count(self._h))
 
+    def generate(self, init: "InitSpec", params: Params) -> None:
+        """Replace the device state by a seeded initial state generated on the device."""
+        c = init.c()
+        raise_for(lib.mhdb_generate(self._h, C.byref(c), C.byref(params)), self._h)
+
     def set_tile_config(self, config: int) -> None:
         raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
 
@@ -250,3 +283,38 @@ def make_params(t_end=0.0, cfl=0.4, gamma=5.0 / 3.0, glm_alpha=0.1, limiter=MC, 
     return Params(float(t_end), float(cfl), float(gamma), float(glm_alpha), int(limiter),
                   int(bool(ohmic)), int(bool(hall)), int(bool(ambipolar)), float(eta_ohm),
                   float(eta_hall), float(eta_ambipolar), int(max_steps))
+
+
+class InitSpec:
+    """Seeded initial state for the device generator: ``fourier(seed)`` or ``quadrants(seed)``
+    (the same draws as workloads.fourier_state / workloads.four_quadrant)."""
+
+    def __init__(self, kind: int, kmax: int = 8, coef=None, quad=None):
+        self.kind = kind
+        self.kmax = kmax
+        self._coef = None
+        if coef is not None:
+            self._coef = np.ascontiguousarray(
+                np.stack([coef.real, coef.imag], axis=-1), dtype=np.float64)
+        self.quad = np.zeros((4, 5)) if quad is None else np.asarray(quad, dtype=np.float64)
+
+    @staticmethod
+    def fourier(seed: int, kmax: int = 8) -> "InitSpec":
+        from .workloads import fourier_coefficients
+        return InitSpec(INIT_FOURIER, kmax, coef=fourier_coefficients(seed, kmax))
+
+    @staticmethod
+    def quadrants(seed: int) -> "InitSpec":
+        from .workloads import quadrant_values
+        return InitSpec(INIT_QUADRANTS, quad=quadrant_values(seed))
+
+    def c(self) -> Init:
+        out = Init()
+        out.kind = self.kind
+        out.kmax = self.kmax
+        out.coef = (self._coef.ctypes.data_as(C.POINTER(C.c_double))
+                    if self._coef is not None else None)
+        for q in range(4):
+            for v in range(5):
+                out.quad[q][v] = float(self.quad[q, v])
+        return out

@@ -17,6 +17,7 @@
 #include "stage_f64.cuh"
 #include "stage_mixed.cuh"
 #include "diagnostics.cuh"
+#include "generate.cuh"
 #include "stage_select.h"
 
 #include <cuda_runtime.h>
@@ -856,6 +857,43 @@ int mhdb_solve_steps(mhdb_solver* h, const mhdb_params* params, int nsteps, mhdb
         return MHDB_INVALID_ARGUMENT;
     }
     return run_solve(h, params, nsteps, result);
+}
+
+int mhdb_generate(mhdb_solver* h, const mhdb_init* init, const mhdb_params* params)
+{
+    return guarded(h, [&] {
+        if (init == nullptr || params == nullptr) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "init and params must not be NULL"};
+        }
+        if (init->kind != MHDB_INIT_FOURIER && init->kind != MHDB_INIT_QUADRANTS) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "unknown initial-state kind"};
+        }
+        if (init->kind == MHDB_INIT_FOURIER && (init->coef == nullptr || init->kmax < 1)) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "Fourier initial state needs kmax >= 1 and coef"};
+        }
+        GenSpec spec{};
+        spec.kind = init->kind;
+        spec.kmax = init->kmax;
+        spec.gamma = params->gamma;
+        std::memcpy(spec.quad, init->quad, sizeof spec.quad);
+        spec.x_min = h->grid.x_min;
+        spec.x_max = h->grid.x_max;
+        spec.y_min = h->grid.y_min;
+        spec.y_max = h->grid.y_max;
+        cudaError_t e;
+        if (h->precision == MHDB_FP64) {
+            e = launch_generate(h->stream, spec, init->coef, h->geom, static_cast<double*>(h->Us),
+                                StoreF64{static_cast<double*>(h->U), h->geom.plane});
+        } else {
+            e = launch_generate(h->stream, spec, init->coef, h->geom, static_cast<double*>(h->Us),
+                                StoreMx{mixed_view(h->U, h->geom), h->geom.plane});
+        }
+        h->launches += init->kind == MHDB_INIT_FOURIER ? 2 : 1;
+        MHDB_CHECK(e);
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        h->last_gm1 = params->gamma - 1.0;
+        h->solved_since_upload = true;
+    });
 }
 
 int mhdb_diagnostics(mhdb_solver* h, const mhdb_params* params, mhdb_diag* out)

@@ -84,6 +84,26 @@ def _synth(coef: np.ndarray, ex: np.ndarray, ey: np.ndarray) -> np.ndarray:
     return np.real(ey.T @ coef @ ex)
 
 
+def fourier_coefficients(seed: int = 0, kmax: int = 8) -> np.ndarray:
+    """The five seeded spectra (vx, vy, A_z, f1, f2) of fourier_state as a complex array of shape
+    (5, 2 kmax + 1, kmax + 1), row ky + kmax, column kx: the input of the device generator."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    modes = _modes(kmax)
+    out = np.zeros((5, 2 * kmax + 1, kmax + 1), dtype=np.complex128)
+    for q in range(5):
+        phases = rng.uniform(0.0, 2.0 * np.pi, size=len(modes))
+        for (kx, ky, kk), ph in zip(modes, phases):
+            out[q, ky + kmax, kx] = kk ** -2.0 * np.exp(1j * ph)
+    return out
+
+
+def quadrant_values(seed: int = 0) -> np.ndarray:
+    """(4, 5) array of (rho, p, vx, vy, By) per quadrant as four_quadrant draws them."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.array([[rng.uniform(0.1, 2.0), rng.uniform(0.1, 2.0), rng.uniform(-1.0, 1.0),
+                      rng.uniform(-1.0, 1.0), rng.uniform(-1.0, 1.0)] for _ in range(4)])
+
+
 def fourier_state(nx: int, ny: int, seed: int = 0, kmax: int = 8, x_min=0.0, x_max=1.0,
                   y_min=0.0, y_max=1.0) -> dict:
     rng = np.random.Generator(np.random.PCG64(seed))
