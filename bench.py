@@ -58,6 +58,13 @@ def parse():
                     help="comma-separated subset of fp64,fp32_mixed (profiling runs)")
     ap.add_argument("--tile-config", type=int, default=-1,
                     help="stage-kernel tile configuration for both forms (-1: autotune)")
+    ap.add_argument("--batch-solves", type=int, default=256,
+                    help="solves of the batched workload (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests of the served stream (0 skips it)")
+    ap.add_argument("--serve-side", default="128,1024")
+    ap.add_argument("--serve-tend", default="0.01,0.05")
     return ap.parse_args()
 
 
@@ -121,6 +128,24 @@ class ClockSampler:
         loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def max_over_ranks(ms: float, dist=None) -> float:
+    """Slowest rank's device time (ms): the whole-job time of a replicas run."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return ms
+    import torch
+
+    backend = dist.get_backend()
+    dev = "cuda" if backend == "nccl" else "cpu"
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(units_per_rank: float, ms_max: float, world: int) -> float:
+    """Whole-job throughput of N replicas: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / (ms_max * 1e-3)
 
 
 def measured_hbm_peak() -> tuple[float, str]:
@@ -187,6 +212,93 @@ def e2e_form(dev, params, host: np.ndarray, calls: int, n: int) -> dict:
     return {"value": float(n) * n * E2E_STEPS * calls / (total * 1e-3), "unit": "zone-updates/s",
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
             "steps_per_call": E2E_STEPS, "calls": calls}
+
+
+def bench_batched(nsolves: int, steps: int, seed: int = 1) -> dict:
+    """256 independent ideal solves, nx and ny each log-uniform in [64, 1024], own seeded Fourier
+    state (generated on the device) and own gamma ~ U[1.4, 5/3], periodic, van Leer, fixed step
+    count, FP32-mixed batch. Also runs the same solves as an FP64 batch (the per-solve L1
+    reference) and one at a time through the single-solve FP32-mixed path."""
+    import math
+
+    import torch
+
+    from mhd_gpu_solver_b200 import _capi
+    from mhd_gpu_solver_b200.batch import BatchSolver, fixed_params
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    solves = []
+    for i in range(nsolves):
+        nx = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        ny = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        solves.append((nx, ny, float(rng.uniform(1.4, 5.0 / 3.0)), int(rng.integers(0, 2**31 - 1))))
+    cells = sum(nx * ny for nx, ny, _, _ in solves)
+
+    def run(precision):
+        b = BatchSolver(precision)
+        ids = [b.add_generated(nx, ny, _capi.InitSpec.fourier(sd),
+                               fixed_params(steps, gamma=g, limiter=_capi.VANLEER), (0, 0),
+                               fixed_steps=True) for nx, ny, g, sd in solves]
+        b.step(2)  # warm-up: kernel attributes, first graph capture
+        # rebuild the same batch and time it from the start
+        b.close()
+        b = BatchSolver(precision)
+        ids = [b.add_generated(nx, ny, _capi.InitSpec.fourier(sd),
+                               fixed_params(steps, gamma=g, limiter=_capi.VANLEER), (0, 0),
+                               fixed_steps=True) for nx, ny, g, sd in solves]
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        while b.step(steps) > 0:
+            pass
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = b.info()["launches"]
+        return b, ids, ms, launches
+
+    bm, idm, ms_m, launches = run(_capi.FP32)
+    b64, id64, ms_64, _ = run(_capi.FP64)
+    errs = []
+    for (nx, ny, g, sd), a, c in zip(solves, idm, id64):
+        um, u64 = bm.download(a), b64.download(c)
+        inner = (slice(None), slice(2, -2), slice(2, -2))
+        num = np.abs(um[inner] - u64[inner]).reshape(9, -1).sum(axis=1)
+        den = np.abs(u64[inner]).reshape(9, -1).sum(axis=1)
+        errs.append(float(np.max((num / np.where(den > 0, den, 1.0))[[0, 1, 2, 4, 5, 6]])))
+    bm.close()
+    b64.close()
+    # one at a time through the single-solve FP32-mixed path
+    t0 = time.perf_counter()
+    for nx, ny, g, sd in solves:
+        dev = _capi.DeviceSolver(nx, ny, precision=_capi.FP32)
+        dev.configure(0, 0)
+        p = _capi.make_params(gamma=g, limiter=_capi.VANLEER)
+        dev.generate(_capi.InitSpec.fourier(sd), p)
+        dev.solve_steps(p, steps)
+        dev.close()
+    one_s = time.perf_counter() - t0
+    return {"workload": f"{nsolves} ideal solves, nx, ny log-uniform in [64,1024], {steps} steps",
+            "cells": cells, "solves_per_s": nsolves / (ms_m * 1e-3),
+            "zone_updates_per_s": cells * steps / (ms_m * 1e-3), "ms": ms_m,
+            "fp64_batch_solves_per_s": nsolves / (ms_64 * 1e-3),
+            "one_at_a_time_fp32_mixed_solves_per_s": nsolves / one_s,
+            "l1_fp32_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "gpu_launches": launches}
+
+
+def bench_served(nreq: int, side, tend) -> dict:
+    from mhd_gpu_solver_b200.serve import make_stream, serve, serve_one_at_a_time
+
+    stream = make_stream(nreq, rate=1e4, seed=2, side=side, t_end=tend, nonideal_frac=0.3)
+    served = serve(stream).summary()
+    plain = serve_one_at_a_time(stream).summary()
+    return {"workload": f"{nreq} requests, Poisson arrivals at 1e4/s (saturating), side "
+                        f"log-uniform in [{side[0]},{side[1]}], t_end ~ U[{tend[0]},{tend[1]}], "
+                        "Fourier or four-quadrant 50/50, 30% non-ideal, FP32-mixed, 150 GB cap",
+            "served": served, "one_at_a_time_fp64": plain,
+            "solves_per_s_ratio": served["solves_per_s"] / plain["solves_per_s"]}
 
 
 def cpu_reference_rate(U: np.ndarray, n: int, steps: int) -> dict:
@@ -295,12 +407,7 @@ def main():
             r["clocks"] = clk.summary()
         else:
             r = time_form(dev, params, args.steps, args.warmup, n)
-        if dist is not None:
-            t = torch.tensor([r["ms"]], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            r["ms_max"] = float(t.item())
-        else:
-            r["ms_max"] = r["ms"]
+        r["ms_max"] = max_over_ranks(r["ms"], dist)
         if name == "fp32_mixed" and args.e2e_calls > 0:
             r["e2e"] = e2e_form(dev, params, host, args.e2e_calls, n)
         dev.close()
@@ -315,7 +422,7 @@ def main():
 
     mixed = results["fp32_mixed"]
     ms = mixed["ms_max"]
-    value = world * float(n) * n * args.steps / (ms * 1e-3)
+    value = replicas_value(float(n) * n * args.steps, ms, world)
     peak, peak_kind = measured_hbm_peak()
     dom = 2 if mixed["prof"]["stage2_ms"] >= mixed["prof"]["stage1_ms"] else 1
     achieved = mixed[f"stage{dom}_gbs"]
@@ -330,7 +437,7 @@ def main():
                    "l2": "state 1.21 GB per buffer >> 126 MB L2, no flush"},
         "tile_configs": {k: next(c for c in _capi.tile_configs(p) if c["config"] == chosen[k])
                          for k, p in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32))},
-        "fp64": {"value": world * float(n) * n * args.steps / (results["fp64"]["ms_max"] * 1e-3),
+        "fp64": {"value": replicas_value(float(n) * n * args.steps, results["fp64"]["ms_max"], world),
                  "ms_per_step": results["fp64"]["ms_max"] / args.steps,
                  "stage1_avg_ms": results["fp64"]["stage1_avg_ms"],
                  "stage2_avg_ms": results["fp64"]["stage2_avg_ms"],
@@ -346,6 +453,12 @@ def main():
         "e2e": mixed.get("e2e"),
         "gpu_launches": mixed["launches"],
     }
+    if rank == 0 and args.batch_solves > 0:
+        line["batched"] = bench_batched(args.batch_solves, args.batch_steps)
+    if rank == 0 and args.serve_requests > 0:
+        side = tuple(int(v) for v in args.serve_side.split(","))
+        tend = tuple(float(v) for v in args.serve_tend.split(","))
+        line["served"] = bench_served(args.serve_requests, side, tend)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference_rate(U, n, args.cpu_steps)

@@ -6,17 +6,18 @@
 
 namespace mhdb {
 
-template <int TX_, int TY_, int NT_, int MINB_>
+template <int TX_, int TY_, int NT_, int MINB_, bool MERGED_ = false>
 struct TileCfg {
     static constexpr int TX = TX_, TY = TY_, NT = NT_, MINB = MINB_;
+    static constexpr bool MERGED = MERGED_;
 };
 
 template <class Policy, class Cfg, int L, bool NI, bool MASK>
 void fill_pair(StageKernels& k)
 {
     using T = typename Policy::T;
-    auto s1 = stage_kernel<Policy, L, NI, MASK, 1, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>;
-    auto s2 = stage_kernel<Policy, L, NI, MASK, 2, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>;
+    auto s1 = stage_kernel<Policy, L, NI, MASK, 1, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB, Cfg::MERGED>;
+    auto s2 = stage_kernel<Policy, L, NI, MASK, 2, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB, Cfg::MERGED>;
     if constexpr (sizeof(T) == 8) {
         k.f64_stage1 = s1;
         k.f64_stage2 = s2;
@@ -27,7 +28,7 @@ void fill_pair(StageKernels& k)
     k.tile_x = Cfg::TX;
     k.tile_y = Cfg::TY;
     k.threads = Cfg::NT;
-    k.smem = stage_smem_bytes<T, Cfg::TX, Cfg::TY, NI>();
+    k.smem = stage_smem_bytes<T, Cfg::TX, Cfg::TY, NI, Cfg::MERGED>();
 }
 
 // Every (limiter, non-ideal, mask) combination for the default configuration.

@@ -4,15 +4,18 @@
 namespace mhdb {
 
 namespace {
-using Cfg0 = TileCfg<32, 8, 256, 2>;  // default
+using Cfg0 = TileCfg<32, 8, 256, 2>; // default
 using Cfg1 = TileCfg<32, 4, 128, 4>;
 using Cfg2 = TileCfg<32, 8, 320, 2>;
-constexpr TileConfigInfo kInfo[] = {{32, 8, 256, 2}, {32, 4, 128, 4}, {32, 8, 320, 2}};
+using Cfg3 = TileCfg<32, 8, 320, 2, true>;
+constexpr TileConfigInfo kInfo[] = {
+    {32, 8, 256, 2, 0}, {32, 4, 128, 4, 0}, {32, 8, 320, 2, 0}, {32, 8, 320, 2, 1}};
+constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
-int stage_config_count_f64() { return 3; }
+int stage_config_count_f64() { return kCount; }
 
-TileConfigInfo stage_config_info_f64(int c) { return kInfo[c < 0 || c > 2 ? 0 : c]; }
+TileConfigInfo stage_config_info_f64(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }
 
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config)
 {
@@ -21,6 +24,8 @@ StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config)
         return select_ideal<PolicyF64, Cfg1>(limiter, nonideal, mask);
     case 2:
         return select_ideal<PolicyF64, Cfg2>(limiter, nonideal, mask);
+    case 3:
+        return select_ideal<PolicyF64, Cfg3>(limiter, nonideal, mask);
     default:
         return select_full<PolicyF64, Cfg0>(limiter, nonideal, mask);
     }

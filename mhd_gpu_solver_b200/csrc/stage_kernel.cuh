@@ -47,34 +47,45 @@ struct TileShape {
     static constexpr int NC = TX * TY;          // owned cells
 };
 
-template <class T, int TX, int TY, bool NI>
+// Shared memory of one tile. Separate sweeps reuse one slope buffer and one flux buffer for x
+// and y; merged sweeps keep x and y buffers side by side.
+template <class T, int TX, int TY, bool NI, bool MERGED = false>
 constexpr size_t stage_smem_bytes()
 {
     using S = TileShape<TX, TY>;
-    return sizeof(T) * (9 * S::NH + 9 * S::SN + 9 * S::NF + (NI ? 3 * S::NJ : 0));
+    const size_t slopes = MERGED ? (S::SXN + S::SYN) : S::SN;
+    const size_t fluxes = MERGED ? (S::NFX + S::NFY) : S::NF;
+    return sizeof(T) * (9 * S::NH + 9 * slopes + 9 * fluxes + (NI ? 3 * S::NJ : 0));
 }
 
-// Slope sweep: for each cell of the sweep region and each component, the limited slope
-// s = lim(W - W_prev, W_next - W) (include/mhd/kernels/muscl_hll.hpp:64-65).
+// One cell of a slope sweep: per component the limited slope s = lim(W - W_prev, W_next - W)
+// (include/mhd/kernels/muscl_hll.hpp:64-65), stored at sS[c * sn + t]. Sweep regions: x: columns
+// 1..TX+2 and rows 2..TY+1 of the halo tile; y: columns 2..TX+1 and rows 1..TY+2.
+template <int L, class T, int TX, int TY, bool YDIR>
+__device__ __forceinline__ void slope_item(const T* __restrict__ sW, T* __restrict__ sS, int sn,
+                                           int t)
+{
+    using S = TileShape<TX, TY>;
+    constexpr int HX = S::HX;
+    constexpr int W = YDIR ? TX : TX + 2;
+    constexpr int step = YDIR ? HX : 1;
+    const int sx = t % W, sy = t / W;
+    const int i = YDIR ? (sy + 1) * HX + (sx + 2) : (sy + 2) * HX + (sx + 1);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        const T* w = sW + c * S::NH + i;
+        const T wm = w[-step], w0 = w[0], wp = w[step];
+        sS[c * sn + t] = limit_slope<L>(w0 - wm, wp - w0);
+    }
+}
+
 template <int L, class T, int TX, int TY, int NT, bool YDIR>
 __device__ __forceinline__ void face_states(const T* __restrict__ sW, T* __restrict__ sS)
 {
     using S = TileShape<TX, TY>;
-    constexpr int HX = S::HX;
-    constexpr int W = YDIR ? TX : TX + 2;       // sweep region width
     constexpr int N = YDIR ? S::SYN : S::SXN;
-    constexpr int step = YDIR ? HX : 1;
     for (int t = threadIdx.x; t < N; t += NT) {
-        const int sx = t % W, sy = t / W;
-        // halo coordinates of the cell (x: columns 1..TX+2, rows 2..TY+1; y: cols 2..TX+1,
-        // rows 1..TY+2)
-        const int i = YDIR ? (sy + 1) * HX + (sx + 2) : (sy + 2) * HX + (sx + 1);
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            const T* w = sW + c * S::NH + i;
-            const T wm = w[-step], w0 = w[0], wp = w[step];
-            sS[c * S::SN + t] = limit_slope<L>(w0 - wm, wp - w0);
-        }
+        slope_item<L, T, TX, TY, YDIR>(sW, sS, S::SN, t);
     }
 }
 
@@ -119,6 +130,55 @@ __device__ __forceinline__ void face_flux(const T* __restrict__ sS, int sn, int 
     out[8] = f.psi;
 }
 
+// One face of a sweep: flux (HLL + GLM + non-ideal E) into sF[c * fn + t]; sS/sn are the
+// slopes of the same sweep (x: region width TX+2; y: width TX).
+template <class T, int TX, int TY, bool YDIR, bool NI>
+__device__ __forceinline__ void face_item(const T* __restrict__ sW, const T* __restrict__ sS,
+                                          int sn, T* __restrict__ sF, int fn,
+                                          const T* __restrict__ sJ, const NonIdealCoef& ni,
+                                          T gamma, T inv_gm1, T c_h, int t)
+{
+    using S = TileShape<TX, TY>;
+    constexpr int HX = S::HX;
+    constexpr int FW = YDIR ? TX : TX + 1;      // faces per row
+    constexpr int SW = YDIR ? TX : TX + 2;      // slope region width
+    const int fx = t % FW, fy = t / FW;
+    // cells left/below (l) and right/above (r) of the face in slope-region coordinates
+    const int ir = YDIR ? (fy + 1) * SW + fx : fy * SW + (fx + 1);
+    const int il = fy * SW + fx;
+    // the same two cells in halo coordinates
+    const int wr = (fy + 2) * HX + (fx + 2);
+    const int wl = wr - (YDIR ? HX : 1);
+    T out[9];
+    face_flux(sS, sn, il, ir, sW, S::NH, wl, wr, YDIR, gamma, inv_gm1, c_h, out);
+    if constexpr (NI) {
+        // Face-averaged J and B, E from Ohm's law (include/mhd/rhs.hpp:75-114).
+        const int jr = (fy + 1) * S::JX + (fx + 1);
+        const int jl = jr - (YDIR ? S::JX : 1);
+        const T Jx = T(0.5) * (sJ[jl] + sJ[jr]);
+        const T Jy = T(0.5) * (sJ[S::NJ + jl] + sJ[S::NJ + jr]);
+        const T Jz = T(0.5) * (sJ[2 * S::NJ + jl] + sJ[2 * S::NJ + jr]);
+        const T Bx = T(0.5) * (sW[5 * S::NH + wl] + sW[5 * S::NH + wr]);
+        const T By = T(0.5) * (sW[6 * S::NH + wl] + sW[6 * S::NH + wr]);
+        const T Bz = T(0.5) * (sW[7 * S::NH + wl] + sW[7 * S::NH + wr]);
+        T Ex, Ey, Ez;
+        nonideal_e(Jx, Jy, Jz, Bx, By, Bz, ni, Ex, Ey, Ez);
+        if (!YDIR) {
+            out[6] += -Ez;
+            out[7] += Ey;
+            out[4] += By * Ez - Bz * Ey;
+        } else {
+            out[5] += Ez;
+            out[7] += -Ex;
+            out[4] += Bz * Ex - Bx * Ez;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        sF[c * fn + t] = out[c];
+    }
+}
+
 // Fluxes of all faces of one sweep into sF, then each owned cell's flux difference into dF.
 template <class T, int TX, int TY, int NT, bool YDIR, bool NI>
 __device__ __forceinline__ void face_sweep(const T* __restrict__ sW, const T* __restrict__ sS,
@@ -127,46 +187,9 @@ __device__ __forceinline__ void face_sweep(const T* __restrict__ sW, const T* __
                                            T (&dF)[(TX * TY + NT - 1) / NT][9])
 {
     using S = TileShape<TX, TY>;
-    constexpr int HX = S::HX;
     constexpr int NFACE = YDIR ? S::NFY : S::NFX;
-    constexpr int FW = YDIR ? TX : TX + 1;      // faces per row
-    constexpr int SW = YDIR ? TX : TX + 2;      // face-state region width
     for (int t = threadIdx.x; t < NFACE; t += NT) {
-        const int fx = t % FW, fy = t / FW;
-        // cells left/below (l) and right/above (r) of the face in face-state coordinates
-        const int ir = YDIR ? (fy + 1) * SW + fx : fy * SW + (fx + 1);
-        const int il = YDIR ? fy * SW + fx : fy * SW + fx;
-        // the same two cells in halo coordinates
-        const int wr = (fy + 2) * HX + (fx + 2);
-        const int wl = wr - (YDIR ? HX : 1);
-        T out[9];
-        face_flux(sS, S::SN, il, ir, sW, S::NH, wl, wr, YDIR, gamma, inv_gm1, c_h, out);
-        if constexpr (NI) {
-            // Face-averaged J and B, E from Ohm's law (include/mhd/rhs.hpp:75-114).
-            const int jr = (fy + 1) * S::JX + (fx + 1);
-            const int jl = jr - (YDIR ? S::JX : 1);
-            const T Jx = T(0.5) * (sJ[jl] + sJ[jr]);
-            const T Jy = T(0.5) * (sJ[S::NJ + jl] + sJ[S::NJ + jr]);
-            const T Jz = T(0.5) * (sJ[2 * S::NJ + jl] + sJ[2 * S::NJ + jr]);
-            const T Bx = T(0.5) * (sW[5 * S::NH + wl] + sW[5 * S::NH + wr]);
-            const T By = T(0.5) * (sW[6 * S::NH + wl] + sW[6 * S::NH + wr]);
-            const T Bz = T(0.5) * (sW[7 * S::NH + wl] + sW[7 * S::NH + wr]);
-            T Ex, Ey, Ez;
-            nonideal_e(Jx, Jy, Jz, Bx, By, Bz, ni, Ex, Ey, Ez);
-            if (!YDIR) {
-                out[6] += -Ez;
-                out[7] += Ey;
-                out[4] += By * Ez - Bz * Ey;
-            } else {
-                out[5] += Ez;
-                out[7] += -Ex;
-                out[4] += Bz * Ex - Bx * Ez;
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            sF[c * S::NF + t] = out[c];
-        }
+        face_item<T, TX, TY, YDIR, NI>(sW, sS, S::SN, sF, S::NF, sJ, ni, gamma, inv_gm1, c_h, t);
     }
     __syncthreads();
 #pragma unroll
@@ -186,7 +209,8 @@ __device__ __forceinline__ void face_sweep(const T* __restrict__ sW, const T* __
 
 // Phases A-E for the tile with lower-left interior cell (x0, y0); returns the largest signal
 // speed of the owned fluid cells after a stage-2 update (0 for stage 1).
-template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT>
+template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT,
+          bool MERGED = false>
 __device__ __forceinline__ double stage_tile(const typename Policy::Args& a, int x0, int y0,
                                              unsigned char* smem_raw)
 {
@@ -255,35 +279,87 @@ __device__ __forceinline__ double stage_tile(const typename Policy::Args& a, int
     __syncthreads();
 
     // B. current J (include/mhd/nonideal.hpp:30-60)
-    if constexpr (NI) {
+    auto current_item = [&](int t) {
         const T inv_2dx = static_cast<T>(k.inv_2dx), inv_2dy = static_cast<T>(k.inv_2dy);
-        for (int t = threadIdx.x; t < S::NJ; t += NT) {
-            const int jx = t % S::JX + 1, jy = t / S::JX + 1;
-            const int i = jy * HX + jx;
-            const T* bx = sW + 5 * S::NH;
-            const T* by = sW + 6 * S::NH;
-            const T* bz = sW + 7 * S::NH;
-            const T dbz_dy = (bz[i + HX] - bz[i - HX]) * inv_2dy;
-            const T dbz_dx = (bz[i + 1] - bz[i - 1]) * inv_2dx;
-            const T dby_dx = (by[i + 1] - by[i - 1]) * inv_2dx;
-            const T dbx_dy = (bx[i + HX] - bx[i - HX]) * inv_2dy;
-            sJ[0 * S::NJ + t] = dbz_dy;
-            sJ[1 * S::NJ + t] = -dbz_dx;
-            sJ[2 * S::NJ + t] = dby_dx - dbx_dy;
+        const int jx = t % S::JX + 1, jy = t / S::JX + 1;
+        const int i = jy * HX + jx;
+        const T* bx = sW + 5 * S::NH;
+        const T* by = sW + 6 * S::NH;
+        const T* bz = sW + 7 * S::NH;
+        const T dbz_dy = (bz[i + HX] - bz[i - HX]) * inv_2dy;
+        const T dbz_dx = (bz[i + 1] - bz[i - 1]) * inv_2dx;
+        const T dby_dx = (by[i + 1] - by[i - 1]) * inv_2dx;
+        const T dbx_dy = (bx[i + HX] - bx[i - HX]) * inv_2dy;
+        sJ[0 * S::NJ + t] = dbz_dy;
+        sJ[1 * S::NJ + t] = -dbz_dx;
+        sJ[2 * S::NJ + t] = dby_dx - dbx_dy;
+    };
+
+    T dFx[R][9];
+    T dGy[R][9];
+    if constexpr (!MERGED) {
+        if constexpr (NI) {
+            for (int t = threadIdx.x; t < S::NJ; t += NT) {
+                current_item(t);
+            }
+        }
+        // C. x sweep
+        face_states<L, T, TX, TY, NT, false>(sW, sS);
+        __syncthreads();
+        face_sweep<T, TX, TY, NT, false, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dFx);
+        __syncthreads();
+        // D. y sweep
+        face_states<L, T, TX, TY, NT, true>(sW, sS);
+        __syncthreads();
+        face_sweep<T, TX, TY, NT, true, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dGy);
+    } else {
+        // Merged sweeps: J, x slopes and y slopes in one flat work list; then x and y faces in
+        // one list (x faces padded to whole warps so that no warp straddles the two kinds).
+        T* sSx = sS;
+        T* sSy = sSx + 9 * S::SXN;
+        T* sFx = sSy + 9 * S::SYN;
+        T* sFy = sFx + 9 * S::NFX;
+        T* sJm = sFy + 9 * S::NFY;
+        sJ = sJm;
+        constexpr int NJI = NI ? S::NJ : 0;
+        for (int t = threadIdx.x; t < NJI + S::SXN + S::SYN; t += NT) {
+            if (t < NJI) {
+                current_item(t);
+            } else if (t < NJI + S::SXN) {
+                slope_item<L, T, TX, TY, false>(sW, sSx, S::SXN, t - NJI);
+            } else {
+                slope_item<L, T, TX, TY, true>(sW, sSy, S::SYN, t - NJI - S::SXN);
+            }
+        }
+        __syncthreads();
+        constexpr int NFXP = (S::NFX + 31) / 32 * 32;
+        for (int t = threadIdx.x; t < NFXP + S::NFY; t += NT) {
+            if (t < NFXP) {
+                if (t < S::NFX) {
+                    face_item<T, TX, TY, false, NI>(sW, sSx, S::SXN, sFx, S::NFX, sJ, k.ni,
+                                                    gamma, inv_gm1, c_h, t);
+                }
+            } else {
+                face_item<T, TX, TY, true, NI>(sW, sSy, S::SYN, sFy, S::NFY, sJ, k.ni, gamma,
+                                               inv_gm1, c_h, t - NFXP);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int t = threadIdx.x + r * NT;
+            if (t < S::NC) {
+                const int cx = t % TX, cy = t / TX;
+                const int fxi = cy * (TX + 1) + cx;
+                const int fyi = cy * TX + cx;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    dFx[r][c] = sFx[c * S::NFX + fxi + 1] - sFx[c * S::NFX + fxi];
+                    dGy[r][c] = sFy[c * S::NFY + fyi + TX] - sFy[c * S::NFY + fyi];
+                }
+            }
         }
     }
-
-    // C. x sweep
-    T dFx[R][9];
-    face_states<L, T, TX, TY, NT, false>(sW, sS);
-    __syncthreads();
-    face_sweep<T, TX, TY, NT, false, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dFx);
-    __syncthreads();
-    // D. y sweep
-    T dGy[R][9];
-    face_states<L, T, TX, TY, NT, true>(sW, sS);
-    __syncthreads();
-    face_sweep<T, TX, TY, NT, true, NI>(sW, sS, sF, sJ, k.ni, gamma, inv_gm1, c_h, dGy);
 
     // E. divergence, psi damping, solid zeroing and the stage update
     const T inv_dx = static_cast<T>(k.inv_dx), inv_dy = static_cast<T>(k.inv_dy);
@@ -314,14 +390,15 @@ __device__ __forceinline__ double stage_tile(const typename Policy::Args& a, int
 }
 
 // One CTA per tile of one grid.
-template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT, int MINB>
+template <class Policy, int L, bool NI, bool MASK, int STAGE, int TX, int TY, int NT, int MINB,
+          bool MERGED = false>
 __global__ void __launch_bounds__(NT, MINB) stage_kernel(const typename Policy::Args a)
 {
     if (a.ctrl->finished != 0) {
         return;
     }
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const double smax = stage_tile<Policy, L, NI, MASK, STAGE, TX, TY, NT>(
+    const double smax = stage_tile<Policy, L, NI, MASK, STAGE, TX, TY, NT, MERGED>(
         a, blockIdx.x * TX, blockIdx.y * TY, smem_raw);
     if constexpr (STAGE == 2) {
         reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
@@ -340,7 +417,8 @@ struct BatchSolve {
 // tile index). Every CTA walks the list with a grid stride; a solve's signal-speed reduction
 // completes when its last tile arrives, whichever CTA processes it, and that tile advances the
 // solve's own FP64 clock. Finished solves are skipped.
-template <class Policy, int L, bool NI, int STAGE, int TX, int TY, int NT, int MINB>
+template <class Policy, int L, bool NI, int STAGE, int TX, int TY, int NT, int MINB,
+          bool MERGED = false>
 __global__ void __launch_bounds__(NT, MINB) batch_stage_kernel(const BatchSolve<Policy>* solves,
                                                               const int2* __restrict__ work,
                                                               int nwork)
@@ -369,7 +447,8 @@ __global__ void __launch_bounds__(NT, MINB) batch_stage_kernel(const BatchSolve<
         }
         const int x0 = (it.y % s_tiles_x) * TX;
         const int y0 = (it.y / s_tiles_x) * TY;
-        const double smax = stage_tile<Policy, L, NI, false, STAGE, TX, TY, NT>(sa, x0, y0, smem_raw);
+        const double smax =
+            stage_tile<Policy, L, NI, false, STAGE, TX, TY, NT, MERGED>(sa, x0, y0, smem_raw);
         if constexpr (STAGE == 2) {
             reduce_signal_speed_and_finish(smax, sa.ctrl, sa.k, static_cast<unsigned>(s_ntiles),
                                            true);

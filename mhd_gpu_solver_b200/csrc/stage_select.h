@@ -23,7 +23,7 @@ struct StageKernels {
 };
 
 struct TileConfigInfo {
-    int tile_x, tile_y, threads, min_blocks;
+    int tile_x, tile_y, threads, min_blocks, merged;
 };
 
 // Number of tile configurations compiled per precision form, and their shapes.

@@ -1,0 +1,200 @@
+"""Serving form: a request loop with continuous batching over the batched solver.
+
+Requests (grid side, initial-state seed and kind, physics parameters, t_end) arrive over time.
+The loop
+
+* admits arrived requests in arrival order while their HBM footprint (two padded FP32-mixed
+  states) fits under the memory cap, generating each initial state directly in HBM (no host
+  state, no upload);
+* advances every admitted, unfinished request together: each chunk of RK2 steps is one
+  persistent launch per stage over all of them, so requests that arrive while others are on the
+  GPU join the next chunk (continuous batching);
+* when a request finishes, downloads its result, frees its memory and records its latency
+  (completion minus arrival).
+
+``serve_one_at_a_time`` runs the same requests through the plain FP64 single-solve path, one after
+the other, as the comparison. ``make_stream`` draws a seeded request stream: Poisson arrivals,
+side log-uniform, t_end uniform, Fourier or four-quadrant states 50/50, and a fraction with
+Ohmic, Hall and ambipolar terms.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from .batch import BatchSolver, state_bytes
+
+# Non-ideal coefficients of the masked 2048^2 workload, reused for non-ideal requests.
+NONIDEAL = dict(ohmic=True, hall=True, ambipolar=True, eta_ohm=1e-3, eta_hall=1e-2,
+                eta_ambipolar=1e-3)
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # seconds after the stream starts
+    n: int                  # square grid side
+    t_end: float
+    kind: str               # "fourier" or "quadrants"
+    seed: int
+    nonideal: bool
+    gamma: float = 5.0 / 3.0
+    limiter: int = _capi.VANLEER
+
+    def params(self) -> _capi.Params:
+        kw = dict(NONIDEAL) if self.nonideal else {}
+        return _capi.make_params(t_end=self.t_end, gamma=self.gamma, limiter=self.limiter, **kw)
+
+    def init(self) -> _capi.InitSpec:
+        return (_capi.InitSpec.fourier(self.seed) if self.kind == "fourier"
+                else _capi.InitSpec.quadrants(self.seed))
+
+    @property
+    def bc(self):
+        return (0, 0) if self.kind == "fourier" else (2, 2)
+
+
+@dataclass
+class Completion:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    steps: int
+    t: float
+    cells: int
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def make_stream(n_requests: int, rate: float, seed: int = 0, side=(128, 2048),
+                t_end=(0.1, 0.5), nonideal_frac: float = 0.3) -> list[Request]:
+    """Seeded request stream: exponential inter-arrival times of mean 1/rate, side log-uniform
+    in [side[0], side[1]], t_end uniform, Fourier or quadrant state with probability 1/2 each,
+    non-ideal terms with probability nonideal_frac."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        n = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1])))))
+        out.append(Request(rid=i, arrival=t, n=n, t_end=float(rng.uniform(*t_end)),
+                           kind="fourier" if rng.uniform() < 0.5 else "quadrants",
+                           seed=int(rng.integers(0, 2**31 - 1)),
+                           nonideal=bool(rng.uniform() < nonideal_frac)))
+    return out
+
+
+@dataclass
+class ServeStats:
+    completions: list = field(default_factory=list)
+    makespan: float = 0.0
+    peak_bytes: int = 0
+    max_active: int = 0
+    chunks: int = 0
+    states: dict = field(default_factory=dict)  # rid -> final state when kept
+
+    def summary(self) -> dict:
+        lat = np.array([c.latency for c in self.completions]) if self.completions else np.zeros(1)
+        zu = float(sum(c.cells * c.steps for c in self.completions))
+        return {"requests": len(self.completions), "makespan_s": self.makespan,
+                "solves_per_s": len(self.completions) / self.makespan if self.makespan else 0.0,
+                "zone_updates_per_s": zu / self.makespan if self.makespan else 0.0,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "peak_hbm_bytes": self.peak_bytes, "max_active": self.max_active,
+                "chunks": self.chunks}
+
+
+def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
+          chunk: int = 16, download: bool = True, keep_states: bool = False) -> ServeStats:
+    """Serve a request stream in real time with continuous batching."""
+    batch = BatchSolver(precision)
+    stats = ServeStats()
+    pending = deque(sorted(requests, key=lambda r: r.arrival))
+    queue: deque[Request] = deque()
+    active: dict[int, tuple[Request, float]] = {}
+    in_use = 0
+    start = time.perf_counter()
+    try:
+        while pending or queue or active:
+            now = time.perf_counter() - start
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            # admission in arrival order while the footprint fits under the cap
+            while queue:
+                req = queue[0]
+                need = state_bytes(req.n, req.n)
+                if in_use + need > memory_cap and active:
+                    break
+                queue.popleft()
+                sid = batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
+                in_use += need
+                active[sid] = (req, time.perf_counter() - start)
+            stats.peak_bytes = max(stats.peak_bytes, in_use)
+            stats.max_active = max(stats.max_active, len(active))
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - start)))
+                continue
+            batch.step(chunk)
+            stats.chunks += 1
+            done_at = time.perf_counter() - start
+            for sid in list(active):
+                r, fin = batch.status(sid)
+                if not fin:
+                    continue
+                req, admitted = active.pop(sid)
+                if download or keep_states:
+                    out = batch.download(sid)
+                    if keep_states:
+                        stats.states[req.rid] = out
+                stats.completions.append(Completion(req.rid, req.arrival, admitted,
+                                                    time.perf_counter() - start if download
+                                                    else done_at, r.steps, r.t,
+                                                    req.n * req.n))
+                batch.remove(sid)
+                in_use -= state_bytes(req.n, req.n)
+        stats.makespan = time.perf_counter() - start
+    finally:
+        batch.close()
+    return stats
+
+
+def serve_one_at_a_time(requests: list[Request], precision: int = _capi.FP64,
+                        download: bool = True, keep_states: bool = False) -> ServeStats:
+    """The same stream through the plain single-solve path, one request at a time, in arrival
+    order (a request waits until it has arrived and the previous one has finished)."""
+    stats = ServeStats()
+    start = time.perf_counter()
+    for req in sorted(requests, key=lambda r: r.arrival):
+        now = time.perf_counter() - start
+        if req.arrival > now:
+            time.sleep(req.arrival - now)
+        admitted = time.perf_counter() - start
+        dev = _capi.DeviceSolver(req.n, req.n, precision=precision)
+        try:
+            dev.configure(*req.bc)
+            params = req.params()
+            dev.generate(req.init(), params)
+            r = dev.solve(params)
+            if download or keep_states:
+                out = dev.download()
+                if keep_states:
+                    stats.states[req.rid] = out
+        finally:
+            dev.close()
+        stats.completions.append(Completion(req.rid, req.arrival, admitted,
+                                            time.perf_counter() - start, r.steps, r.t,
+                                            req.n * req.n))
+        stats.max_active = 1
+    stats.makespan = time.perf_counter() - start
+    return stats

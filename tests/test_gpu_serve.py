@@ -1,0 +1,44 @@
+"""Serving form: requests that arrive while others run are admitted under the memory cap, all
+complete, and each result is the same alone and in the mix (bit for bit), and within the FP32-mixed
+tolerance of the plain FP64 path."""
+
+import numpy as np
+import pytest
+
+from mhd_gpu_solver_b200 import _capi
+from mhd_gpu_solver_b200.batch import state_bytes
+from mhd_gpu_solver_b200.serve import make_stream, serve, serve_one_at_a_time
+from tests.helpers import rel_l1
+
+pytestmark = pytest.mark.gpu
+
+
+def small_stream(n=12, seed=5):
+    return make_stream(n, rate=400.0, seed=seed, side=(40, 160), t_end=(0.005, 0.02),
+                       nonideal_frac=0.3)
+
+
+def test_served_results_equal_alone_and_fp64_path():
+    reqs = small_stream()
+    mixed = serve(reqs, keep_states=True)
+    assert len(mixed.completions) == len(reqs)
+    assert mixed.max_active > 1  # requests overlapped on the device
+    for req in reqs:
+        alone = serve([req], keep_states=True)
+        assert np.array_equal(alone.states[req.rid], mixed.states[req.rid]), req
+    plain = serve_one_at_a_time(reqs, keep_states=True)
+    steps_mixed = {c.rid: c.steps for c in mixed.completions}
+    for c in plain.completions:
+        assert abs(steps_mixed[c.rid] - c.steps) <= 1
+        err = rel_l1(mixed.states[c.rid], plain.states[c.rid])
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= 1e-6), (c.rid, err)
+
+
+def test_admission_respects_the_memory_cap():
+    reqs = small_stream(10, seed=9)
+    cap = 2.5 * max(state_bytes(r.n, r.n) for r in reqs)
+    stats = serve(reqs, memory_cap=cap)
+    assert len(stats.completions) == len(reqs)
+    assert stats.peak_bytes <= cap
+    s = stats.summary()
+    assert s["p99_ms"] >= s["p50_ms"] > 0.0
