@@ -56,8 +56,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="fp64,fp32_mixed",
                     help="comma-separated subset of fp64,fp32_mixed (profiling runs)")
-    ap.add_argument("--tile-config", type=int, default=-1,
-                    help="stage-kernel tile configuration for both forms (-1: autotune)")
+    ap.add_argument("--tile-config", default="-1",
+                    help="stage-kernel tile configuration, one value for both forms or "
+                         "'fp64,fp32_mixed' (-1: autotune)")
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
+                    help="CPU time bound of the reference arm's timed sample")
     ap.add_argument("--batch-solves", type=int, default=256,
                     help="solves of the batched workload (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=200)
@@ -335,16 +338,20 @@ def run_reference_arm(args, rank: int) -> None:
                    fixed_steps=True)
     p.max_steps = max(1, args.warmup)
     state, *_ = orc.solve(U, orc.Grid(n, n), p, impl="ref")
-    p.max_steps = args.steps
+    # Bound the timed sample: as many of the K steps as fit in --ref-seconds at the warm-up rate.
+    per_step = orc.ref_last_loop_seconds() / p.max_steps
+    timed = max(1, min(args.steps, int(args.ref_seconds / max(per_step, 1e-9))))
+    p.max_steps = timed
     orc.solve(state, orc.Grid(n, n), p, impl="ref")
     dt = orc.ref_last_loop_seconds()
-    value = float(n) * n * args.steps / dt
-    sample = (f"{args.steps} SSP-RK2 steps of the {n}^2 periodic Fourier state after "
+    value = float(n) * n * timed / dt
+    sample = (f"{timed} of the {args.steps} requested SSP-RK2 steps (bounded to about "
+              f"{args.ref_seconds:.0f} s of CPU work) of the {n}^2 periodic Fourier state after "
               f"{args.warmup} warm-up steps, step loop timed alone, MC limiter (no van Leer in "
               f"the reference), {orc.ref_simd_backend()}, {threads} threads")
     line = {"metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
             "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "warmup": args.warmup, "steps_timed": timed, "ms_per_step": dt * 1e3 / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"fourier_periodic_{n}x{n}", "grid": [n, n],
@@ -389,8 +396,10 @@ def main():
     from mhd_gpu_solver_b200 import autotune
 
     chosen = {}
+    cfgs = [int(v) for v in args.tile_config.split(",")]
+    cfg_of = {"fp64": cfgs[0], "fp32_mixed": cfgs[-1]}
     for name, prec in forms:
-        cfg = args.tile_config
+        cfg = cfg_of[name]
         if cfg < 0:
             cfg = autotune.tune(prec, _capi.VANLEER, n, n)
         chosen[name] = cfg

@@ -157,11 +157,16 @@ long long mhdb_launch_count(const mhdb_solver* h);
 
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the default) serves every
    solve; the others exist for ideal solves without a mask and are picked per grid size class by
-   the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes tile width, tile
-   height, threads per CTA and the minimum CTAs per SM of one configuration. */
+   the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells
+   one CTA covers (tile width and height), threads per CTA and the minimum CTAs per SM of one
+   configuration; mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile,
+   separate x and y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps) or MHDB_KERNEL_MARCH (warp
+   strip march, 28 columns per warp), or -1 for an unknown configuration. */
+enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2 };
 int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);
+int mhdb_tile_config_kind(int precision, int config);
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
 /* ---------------------------------------------------------------- batched form (additive)

@@ -26,10 +26,10 @@ EXPORTS = (
     "mhdb_precision", "mhdb_configure", "mhdb_upload", "mhdb_download", "mhdb_solve",
     "mhdb_solve_steps", "mhdb_diagnostics", "mhdb_stream", "mhdb_set_profiling",
     "mhdb_profile_read", "mhdb_launch_count", "mhdb_tile_config_count", "mhdb_tile_config_info",
-    "mhdb_set_tile_config", "mhdb_solve_steps_noalloc_f64", "mhdb_batch_create",
-    "mhdb_batch_destroy", "mhdb_batch_last_error", "mhdb_batch_add", "mhdb_batch_remove",
-    "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download", "mhdb_batch_info",
-    "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
+    "mhdb_tile_config_kind", "mhdb_set_tile_config", "mhdb_solve_steps_noalloc_f64",
+    "mhdb_batch_create", "mhdb_batch_destroy", "mhdb_batch_last_error", "mhdb_batch_add",
+    "mhdb_batch_remove", "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download",
+    "mhdb_batch_info", "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
 )
 
 
@@ -96,6 +96,7 @@ def _load() -> C.CDLL:
         "mhdb_tile_config_count": ([C.c_int], C.c_int),
         "mhdb_tile_config_info": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "mhdb_tile_config_kind": ([C.c_int, C.c_int], C.c_int),
         "mhdb_set_tile_config": ([h, C.c_int], C.c_int),
         "mhdb_solve_steps_noalloc_f64": ([C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(Params),
                                           C.c_int, C.c_void_p, C.c_void_p, C.POINTER(Result),
@@ -267,13 +268,17 @@ class DeviceSolver:
         raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
 
 
+KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march"}
+
+
 def tile_configs(precision: int) -> list[dict]:
     out = []
     for c in range(lib.mhdb_tile_config_count(int(precision))):
         v = [C.c_int() for _ in range(4)]
         raise_for(lib.mhdb_tile_config_info(int(precision), c, *[C.byref(x) for x in v]), None)
         out.append({"config": c, "tile_x": v[0].value, "tile_y": v[1].value,
-                    "threads": v[2].value, "min_blocks": v[3].value})
+                    "threads": v[2].value, "min_blocks": v[3].value,
+                    "kind": KERNEL_KINDS[lib.mhdb_tile_config_kind(int(precision), c)]})
     return out
 
 

@@ -1,6 +1,9 @@
 // Instantiation helpers shared by kernels_f64.cu and kernels_mixed.cu.
 #pragma once
 
+#include <type_traits>
+
+#include "march_kernel.cuh"
 #include "stage_kernel.cuh"
 #include "stage_select.h"
 
@@ -13,7 +16,7 @@ struct TileCfg {
 };
 
 template <class Policy, class Cfg, int L, bool NI, bool MASK>
-void fill_pair(StageKernels& k)
+void fill_pair_tile(StageKernels& k)
 {
     using T = typename Policy::T;
     auto s1 = stage_kernel<Policy, L, NI, MASK, 1, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB, Cfg::MERGED>;
@@ -29,6 +32,45 @@ void fill_pair(StageKernels& k)
     k.tile_y = Cfg::TY;
     k.threads = Cfg::NT;
     k.smem = stage_smem_bytes<T, Cfg::TX, Cfg::TY, NI, Cfg::MERGED>();
+    k.smem2 = k.smem;
+}
+
+// Strip-march configuration: NW warps per block, LY rows per warp, MINB blocks per SM.
+template <int NW_, int LY_, int MINB_>
+struct MarchCfg {
+    static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
+    static constexpr bool MARCH = true;
+};
+
+template <class Cfg, class = void>
+struct is_march : std::false_type {};
+template <class Cfg>
+struct is_march<Cfg, std::void_t<decltype(Cfg::MARCH)>> : std::true_type {};
+
+template <class Policy, class Cfg, int L, bool NI, bool MASK>
+void fill_pair(StageKernels& k)
+{
+    if constexpr (is_march<Cfg>::value) {
+        static_assert(!NI && !MASK, "the strip-march kernel serves ideal, unmasked solves");
+        using T = typename Policy::T;
+        auto s1 = march_kernel<Policy, L, 1, Cfg::LY, Cfg::NW, Cfg::MINB>;
+        auto s2 = march_kernel<Policy, L, 2, Cfg::LY, Cfg::NW, Cfg::MINB>;
+        if constexpr (sizeof(T) == 8) {
+            k.f64_stage1 = s1;
+            k.f64_stage2 = s2;
+        } else {
+            k.mx_stage1 = s1;
+            k.mx_stage2 = s2;
+        }
+        k.tile_x = Cfg::NW * kMarchOwned;
+        k.tile_y = Cfg::LY;
+        k.threads = Cfg::NW * 32;
+        k.smem = 0;
+        k.smem2 = 0;
+        return;
+    } else {
+        fill_pair_tile<Policy, Cfg, L, NI, MASK>(k);
+    }
 }
 
 // Every (limiter, non-ideal, mask) combination for the default configuration.

@@ -8,8 +8,11 @@ using Cfg0 = TileCfg<32, 8, 256, 2>; // default
 using Cfg1 = TileCfg<32, 4, 128, 4>;
 using Cfg2 = TileCfg<32, 8, 320, 2>;
 using Cfg3 = TileCfg<32, 8, 320, 2, true>;
-constexpr TileConfigInfo kInfo[] = {
-    {32, 8, 256, 2, 0}, {32, 4, 128, 4, 0}, {32, 8, 320, 2, 0}, {32, 8, 320, 2, 1}};
+using Cfg4 = MarchCfg<4, 64, 2>;
+using Cfg5 = MarchCfg<4, 64, 3>;
+constexpr TileConfigInfo kInfo[] = {{32, 8, 256, 2, kKindTile},    {32, 4, 128, 4, kKindTile},
+                                    {32, 8, 320, 2, kKindTile},    {32, 8, 320, 2, kKindTileMerged},
+                                    {112, 64, 128, 2, kKindMarch}, {112, 64, 128, 3, kKindMarch}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -26,6 +29,10 @@ StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config)
         return select_ideal<PolicyF64, Cfg2>(limiter, nonideal, mask);
     case 3:
         return select_ideal<PolicyF64, Cfg3>(limiter, nonideal, mask);
+    case 4:
+        return select_ideal<PolicyF64, Cfg4>(limiter, nonideal, mask);
+    case 5:
+        return select_ideal<PolicyF64, Cfg5>(limiter, nonideal, mask);
     default:
         return select_full<PolicyF64, Cfg0>(limiter, nonideal, mask);
     }

@@ -10,8 +10,16 @@ using Cfg2 = TileCfg<32, 8, 256, 3>;
 using Cfg3 = TileCfg<32, 16, 384, 2, true>;
 using Cfg4 = TileCfg<32, 16, 256, 2, true>;
 using Cfg5 = TileCfg<32, 8, 320, 3, true>;
-constexpr TileConfigInfo kInfo[] = {{32, 16, 256, 2, 0}, {32, 16, 256, 3, 0}, {32, 8, 256, 3, 0},
-                                    {32, 16, 384, 2, 1}, {32, 16, 256, 2, 1}, {32, 8, 320, 3, 1}};
+using Cfg6 = MarchCfg<4, 64, 4>;
+using Cfg7 = MarchCfg<4, 32, 4>;
+using Cfg8 = MarchCfg<4, 128, 4>;
+using Cfg9 = MarchCfg<4, 64, 3>;
+constexpr TileConfigInfo kInfo[] = {
+    {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
+    {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
+    {32, 16, 256, 2, kKindTileMerged}, {32, 8, 320, 3, kKindTileMerged},
+    {112, 64, 128, 4, kKindMarch},     {112, 32, 128, 4, kKindMarch},
+    {112, 128, 128, 4, kKindMarch},    {112, 64, 128, 3, kKindMarch}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -32,6 +40,14 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_ideal<PolicyMixed, Cfg4>(limiter, nonideal, mask);
     case 5:
         return select_ideal<PolicyMixed, Cfg5>(limiter, nonideal, mask);
+    case 6:
+        return select_ideal<PolicyMixed, Cfg6>(limiter, nonideal, mask);
+    case 7:
+        return select_ideal<PolicyMixed, Cfg7>(limiter, nonideal, mask);
+    case 8:
+        return select_ideal<PolicyMixed, Cfg8>(limiter, nonideal, mask);
+    case 9:
+        return select_ideal<PolicyMixed, Cfg9>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

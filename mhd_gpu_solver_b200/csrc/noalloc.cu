@@ -172,7 +172,7 @@ int mhdb_solve_steps_noalloc_f64(const mhdb_grid* grid, int bc_x, int bc_y,
                (params->ambipolar && params->eta_ambipolar != 0.0);
 
     const StageKernels sk = select_stage_f64(params->limiter, k.ni_any != 0, false, 0);
-    if (sk.smem == 0) {
+    if (sk.threads == 0) {
         return fail(MHDB_INVALID_ARGUMENT, "no stage kernel for this configuration");
     }
 

@@ -24,6 +24,36 @@ struct FluxN {
     T rho, mn, mt, mz, e, bn, bt, bz, psi;
 };
 
+// Reciprocal and square root. FP64: IEEE division and sqrt, as the reference computes them.
+// FP32 (the FP32-mixed form): the hardware approximations rcp.approx.ftz / sqrt.approx.ftz (PTX
+// ISA; about 1 ulp), used only where the operand is a positive normal number or the result is
+// discarded by a select (inverse densities, 1/(sR - sL) with sR - sL >= 2 c_h, |B|, the van
+// Leer denominator a + b with ab > 0, and the non-negative fast-speed discriminants).
+template <class T>
+__device__ __forceinline__ T fast_rcp(T x)
+{
+    return T(1) / x;
+}
+template <>
+__device__ __forceinline__ float fast_rcp<float>(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+template <class T>
+__device__ __forceinline__ T fast_sqrt(T x)
+{
+    return sqrt(x);
+}
+template <>
+__device__ __forceinline__ float fast_sqrt<float>(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // mhd::simd scalar min/max (include/mhd/simd.hpp:40-47): the first operand wins ties and
 // NaN comparisons, exactly as (b < a) ? b : a.
 template <class T>
@@ -35,6 +65,18 @@ template <class T>
 __device__ __forceinline__ T vmax(T a, T b)
 {
     return (a < b) ? b : a;
+}
+// FP32 (the FP32-mixed form): the single-instruction IEEE minNum/maxNum, which agree with the
+// reference's selection for every pair of numbers and differ only in which operand a NaN yields.
+template <>
+__device__ __forceinline__ float vmin<float>(float a, float b)
+{
+    return fminf(a, b);
+}
+template <>
+__device__ __forceinline__ float vmax<float>(float a, float b)
+{
+    return fmaxf(a, b);
 }
 
 template <class T>
@@ -64,6 +106,16 @@ __device__ __forceinline__ T vanleer_limiter(T a, T b)
 {
     return (a * b <= T(0)) ? T(0) : (T(2) * a * b) / (a + b);
 }
+// FP32: 2ab * rcp(a + b) without a branch. When ab > 0 after rounding, a and b share their sign
+// and max(|a|, |b|) >= 2^-74.5, so a + b is a normal number and the approximate reciprocal is
+// within its stated error; otherwise the select returns 0.
+template <>
+__device__ __forceinline__ float vanleer_limiter<float>(float a, float b)
+{
+    const float p = a * b;
+    const float q = (p + p) * fast_rcp(a + b);
+    return (p <= 0.0f) ? 0.0f : q;
+}
 
 template <int L, class T>
 __device__ __forceinline__ T limit_slope(T a, T b)
@@ -91,7 +143,7 @@ __device__ __forceinline__ void reconstruct(T wmm, T wm, T w0, T wp, T& left, T&
 template <class T>
 __device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
 {
-    const T inv_rho = T(1) / W.rho;
+    const T inv_rho = fast_rcp(W.rho);
     const T cs2 = gamma * W.p * inv_rho;
     const T bn2 = W.bn * W.bn;
     const T b2 = bn2 + W.bt * W.bt + W.bz * W.bz;
@@ -99,8 +151,8 @@ __device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
     const T van2 = bn2 * inv_rho;
     const T sum = cs2 + va2;
     const T disc = vmax(sum * sum - T(4) * cs2 * van2, T(0));
-    const T cf2 = T(0.5) * (sum + sqrt(disc));
-    return sqrt(vmax(cf2, T(0)));
+    const T cf2 = T(0.5) * (sum + fast_sqrt(disc));
+    return fast_sqrt(vmax(cf2, T(0)));
 }
 
 // Conserved state and GLM-MHD flux along n; include/mhd/kernels/muscl_hll.hpp:89-124.
@@ -156,19 +208,44 @@ __device__ __forceinline__ FluxN<T> hll_flux(const PrimN<T>& WL, const PrimN<T>&
     conserved_and_flux(WR, inv_gm1, ch2, UR, FR);
 
     const T denom = sR - sL;
-    const T inv_denom = T(1) / denom;
+    const T inv_denom = fast_rcp(denom);
     const T sLsR = sL * sR;
     const bool use_left = sL >= T(0);
     const bool use_right = sR <= T(0);
     const bool degenerate = fabs(denom) < T(1.0e-14);
 
+    // FP64: the reference's operation order. FP32: the three weights folded into 1/(sR - sL)
+    // once per face, four operations per component.
+    const T wR = sR * inv_denom, wL = sL * inv_denom, wLR = sLsR * inv_denom;
+    auto hll = [&](T fl, T fr, T ul, T ur) {
+        if constexpr (sizeof(T) == 4) {
+            return wR * fl - wL * fr + wLR * (ur - ul);
+        } else {
+            return (sR * fl - sL * fr + sLsR * (ur - ul)) * inv_denom;
+        }
+    };
     auto combine = [&](T fl, T fr, T ul, T ur) {
-        const T hll = (sR * fl - sL * fr + sLsR * (ur - ul)) * inv_denom;
-        const T mid = degenerate ? T(0.5) * (fl + fr) : hll;
+        const T mid = degenerate ? T(0.5) * (fl + fr) : hll(fl, fr, ul, ur);
         return use_left ? fl : (use_right ? fr : mid);
     };
 
     FluxN<T> F;
+    if (c_h >= T(1.0e-14)) {
+        // sL <= -c_h < 0 < c_h <= sR (or NaN) and sR - sL >= 2 c_h > 1e-14: neither upwind
+        // branch nor the degenerate one can be taken, so the selection below returns the HLL
+        // average for every component (NaN included). c_h is the same for every face of a
+        // launch, so this branch does not diverge.
+        F.rho = hll(FL.rho, FR.rho, UL.rho, UR.rho);
+        F.mn = hll(FL.mn, FR.mn, UL.mn, UR.mn);
+        F.mt = hll(FL.mt, FR.mt, UL.mt, UR.mt);
+        F.mz = hll(FL.mz, FR.mz, UL.mz, UR.mz);
+        F.e = hll(FL.e, FR.e, UL.e, UR.e);
+        F.bn = hll(FL.bn, FR.bn, UL.bn, UR.bn);
+        F.bt = hll(FL.bt, FR.bt, UL.bt, UR.bt);
+        F.bz = hll(FL.bz, FR.bz, UL.bz, UR.bz);
+        F.psi = hll(FL.psi, FR.psi, UL.psi, UR.psi);
+        return F;
+    }
     F.rho = combine(FL.rho, FR.rho, UL.rho, UR.rho);
     F.mn = combine(FL.mn, FR.mn, UL.mn, UR.mn);
     F.mt = combine(FL.mt, FR.mt, UL.mt, UR.mt);
@@ -186,7 +263,7 @@ template <class T>
 __device__ __forceinline__ T cell_max_signal_speed(T rho, T mx, T my, T mz, T energy, T bx, T by,
                                                    T bz, T gamma)
 {
-    const T inv_rho = T(1) / rho;
+    const T inv_rho = fast_rcp(rho);
     PrimN<T> W;
     W.rho = rho;
     W.vn = mx * inv_rho;
@@ -216,7 +293,7 @@ __device__ __forceinline__ void cons_to_prim(const T* u, T gm1, T* w)
 {
     const T rho = u[0], mx = u[1], my = u[2], mz = u[3], e = u[4];
     const T bx = u[5], by = u[6], bz = u[7];
-    const T inv_rho = T(1) / rho;
+    const T inv_rho = fast_rcp(rho);
     const T ekin = T(0.5) * (mx * mx + my * my + mz * mz) * inv_rho;
     const T emag = T(0.5) * (bx * bx + by * by + bz * bz);
     w[0] = rho;
@@ -316,7 +393,7 @@ __device__ __forceinline__ void nonideal_e(T Jx, T Jy, T Jz, T Bx, T By, T Bz,
     const T cy = Jz * Bx - Jx * Bz;
     const T cz = Jx * By - Jy * Bx;
     if (c.hall) {
-        const T invB = T(1) / sqrt(B2);
+        const T invB = fast_rcp(fast_sqrt(B2));
         const T eh = T(c.eta_hall);
         Ex += eh * cx * invB;
         Ey += eh * cy * invB;
@@ -326,7 +403,7 @@ __device__ __forceinline__ void nonideal_e(T Jx, T Jy, T Jz, T Bx, T By, T Bz,
         const T dx = cy * Bz - cz * By;
         const T dy = cz * Bx - cx * Bz;
         const T dz = cx * By - cy * Bx;
-        const T invB2 = T(1) / B2;
+        const T invB2 = fast_rcp(B2);
         const T ea = T(c.eta_ambipolar);
         Ex += ea * dx * invB2;
         Ey += ea * dy * invB2;

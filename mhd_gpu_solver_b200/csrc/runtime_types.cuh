@@ -29,7 +29,9 @@ struct Consts {
     int ni_any;
 };
 
-enum CtrlStatus : int { kStatusBadDt = 1 };
+// kStatusWaitTimeout: a stage kernel gave up waiting for one of its own bulk copies (bounded
+// wait); the solve stops and the host reports it as a CUDA error.
+enum CtrlStatus : int { kStatusBadDt = 1, kStatusWaitTimeout = 2 };
 
 // Device-resident time control (FP64 clock). Written only by the last CTA of the stage-2 (or
 // initial CFL) kernel, read by every CTA of the following launches.
@@ -73,7 +75,8 @@ __device__ __forceinline__ void finish_step(Ctrl* ctrl, const Consts& k, bool ad
         ctrl->t += ctrl->dt;
         ctrl->steps += 1;
     }
-    if (!(ctrl->t < ctrl->t_end) || ctrl->steps >= ctrl->max_steps) {
+    if (!(ctrl->t < ctrl->t_end) || ctrl->steps >= ctrl->max_steps ||
+        (ctrl->status & kStatusWaitTimeout) != 0) {
         ctrl->finished = 1;
         return;
     }

@@ -331,7 +331,7 @@ struct StepPlan {
     StageFnMx m1 = nullptr, m2 = nullptr;
     StageArgsMx b1{}, b2{};
     dim3 grid, block;
-    size_t smem = 0;
+    size_t smem = 0, smem2 = 0; // dynamic shared memory of stage 1 and stage 2
     Consts k{};
 };
 
@@ -365,18 +365,20 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
         s.b2 = StageArgsMx{us, u, h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
                            h->walls ? 1 : 0};
     }
-    if (sk.smem == 0) {
+    if (sk.threads == 0) {
         throw ApiError{MHDB_INVALID_ARGUMENT, "no stage kernel for this configuration"};
     }
     s.grid = dim3((h->grid.nx + sk.tile_x - 1) / sk.tile_x, (h->grid.ny + sk.tile_y - 1) / sk.tile_y);
     s.block = dim3(sk.threads);
     s.smem = sk.smem;
+    s.smem2 = sk.smem2;
+    const int b1 = static_cast<int>(s.smem), b2 = static_cast<int>(s.smem2);
     if (!s.mixed) {
-        MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
-        MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+        MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
     } else {
-        MHDB_CHECK(cudaFuncSetAttribute(s.m1, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
-        MHDB_CHECK(cudaFuncSetAttribute(s.m2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(s.smem)));
+        MHDB_CHECK(cudaFuncSetAttribute(s.m1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+        MHDB_CHECK(cudaFuncSetAttribute(s.m2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
     }
     return s;
 }
@@ -384,9 +386,11 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
 void launch_stage(mhdb_solver* h, const StepPlan& s, int stage)
 {
     if (!s.mixed) {
-        (stage == 1 ? s.s1 : s.s2)<<<s.grid, s.block, s.smem, h->stream>>>(stage == 1 ? s.a1 : s.a2);
+        (stage == 1 ? s.s1 : s.s2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
+            stage == 1 ? s.a1 : s.a2);
     } else {
-        (stage == 1 ? s.m1 : s.m2)<<<s.grid, s.block, s.smem, h->stream>>>(stage == 1 ? s.b1 : s.b2);
+        (stage == 1 ? s.m1 : s.m2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
+            stage == 1 ? s.b1 : s.b2);
     }
     ++h->launches;
 }
@@ -624,6 +628,9 @@ int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result
             }
         }
         const Ctrl& c = *h->ctrl_host;
+        if ((c.status & kStatusWaitTimeout) != 0) {
+            throw ApiError{MHDB_CUDA_ERROR, "stage kernel: a bulk-copy wait exceeded its limit"};
+        }
         if ((c.status & kStatusBadDt) != 0) {
             throw ApiError{MHDB_BAD_TIMESTEP, "ssp_rk2_step requires positive dt"};
         }
@@ -998,6 +1005,15 @@ int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, i
     if (threads) *threads = t.threads;
     if (min_blocks) *min_blocks = t.min_blocks;
     return MHDB_OK;
+}
+
+int mhdb_tile_config_kind(int precision, int config)
+{
+    if (config < 0 || config >= mhdb_tile_config_count(precision)) {
+        return -1;
+    }
+    return (precision == MHDB_FP32 ? stage_config_info_mixed(config)
+                                   : stage_config_info_f64(config)).kind;
 }
 
 int mhdb_set_tile_config(mhdb_solver* h, int config)

@@ -72,7 +72,6 @@ struct PolicyF64 {
     struct Raw {
         double v[9];
     };
-
     static __device__ __forceinline__ void load_raw(const Args& a, const Geometry& g, int x, int y,
                                                     Raw& r)
     {
@@ -117,31 +116,61 @@ struct PolicyF64 {
                 L[c] = 0.0;
             }
         }
-        double uin[9];
         if (solid && a.walls) {
+            double uin[9];
             wall_fill_f64(a.uin, a.mask, g, gx, gy, k.gm1, uin);
-        } else {
-            load_cons_f64(a.uin, g, gx, gy, uin);
+            // a solid cell's stored U* is the fill of U^n and U^n is the stage input
+            update_ops<STAGE>(a, g, gx, gy, solid, L, dt, k, smax, [&](int i) {
+                return i < 9 ? uin[i] : __ldg(a.uin + static_cast<size_t>(i - 9) * g.plane +
+                                              static_cast<size_t>(gy) * g.pitch + gx);
+            });
+            return;
         }
         const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        const double* __restrict__ in = a.uin + o;
+        // the stored U* of a solid cell (stage 2 input) stands in for its U^n
+        const double* __restrict__ un = (solid ? a.uin : a.out) + o;
+        const size_t pl = g.plane;
+        update_ops<STAGE>(a, g, gx, gy, solid, L, dt, k, smax, [&](int i) {
+            return i < 9 ? __ldg(in + static_cast<size_t>(i) * pl)
+                         : un[static_cast<size_t>(i - 9) * pl];
+        });
+    }
+
+    // The stage update of one cell from its own-cell operands op(i): plane i of the input (i < 9)
+    // and, in stage 2, plane i - 9 of U^n (i < 18), which the stage overwrites; all are read
+    // before any store.
+    template <int STAGE, class Op>
+    static __device__ __forceinline__ void update_ops(const Args& a, const Geometry& g, int gx,
+                                                      int gy, bool solid, const double (&L)[9],
+                                                      double dt, const Consts& k, double& smax,
+                                                      const Op& op)
+    {
+        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        double* __restrict__ out = a.out + o;
+        const size_t pl = g.plane;
+        double uin[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            uin[c] = op(c);
+        }
         if constexpr (STAGE == 1) {
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
-                a.out[static_cast<size_t>(c) * g.plane + o] = uin[c] + dt * L[c];
+                out[c * pl] = uin[c] + dt * L[c];
             }
         } else {
             double un[9];
-            if (solid) {
-                load_cons_f64(a.uin, g, gx, gy, un);
-            } else {
-                load_cons_f64(a.out, g, gx, gy, un);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                un[c] = op(9 + c);
             }
             const double half_dt = 0.5 * dt;
             double r2[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 r2[c] = 0.5 * (un[c] + uin[c]) + half_dt * L[c];
-                a.out[static_cast<size_t>(c) * g.plane + o] = r2[c];
+                out[c * pl] = r2[c];
             }
             if (!solid) {
                 smax = vmax(smax, signal_speed(r2, k));

@@ -89,45 +89,61 @@ __device__ __forceinline__ void face_states(const T* __restrict__ sW, T* __restr
     }
 }
 
-// One face flux from the slopes and centre values of its two cells: left state W(l) + s(l)/2,
-// right state W(r) - s(r)/2 (include/mhd/kernels/muscl_hll.hpp:66-67), with the both-sides
-// first-order fallback of muscl_hll.hpp:145-168. Output in physical component order.
-template <class T>
-__device__ __forceinline__ void face_flux(const T* __restrict__ sS, int sn, int il, int ir,
-                                          const T* __restrict__ sW, int nh, int wl, int wr,
-                                          bool ydir, T gamma, T inv_gm1, T c_h, T* out)
+// One face flux from the centre values lc, rc and limited slopes sl, sr (physical component
+// order) of its two cells: left state W(l) + s(l)/2, right state W(r) - s(r)/2
+// (include/mhd/kernels/muscl_hll.hpp:66-67), with the both-sides first-order fallback of
+// muscl_hll.hpp:145-168. Output in physical component order.
+template <class T, bool YDIR>
+__device__ __forceinline__ void face_flux_regs(const T (&lc)[9], const T (&sl)[9],
+                                               const T (&rc)[9], const T (&sr)[9], T gamma,
+                                               T inv_gm1, T c_h, T (&out)[9])
 {
     // physical component feeding each rotated-frame slot (rho, vn, vt, vz, p, bn, bt, bz, psi)
-    int comp[9] = {0, ydir ? 2 : 1, ydir ? 1 : 2, 3, 4, ydir ? 6 : 5, ydir ? 5 : 6, 7, 8};
-    T l[9], r[9], lc[9], rc[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const int c = comp[q];
-        lc[q] = sW[c * nh + wl];
-        rc[q] = sW[c * nh + wr];
-        l[q] = lc[q] + T(0.5) * sS[c * sn + il];
-        r[q] = rc[q] - T(0.5) * sS[c * sn + ir];
-    }
+    constexpr int comp[9] = {0, YDIR ? 2 : 1, YDIR ? 1 : 2, 3, 4, YDIR ? 6 : 5, YDIR ? 5 : 6, 7, 8};
+    // Density and pressure of both states decide the fallback; then every component is
+    // W + h s with h = 1/2 (second order) or h = 0 (first order: W + 0 s = W exactly for finite
+    // slopes, and 0.5 s is exact, so both cases give the reference's values).
     const T inf = T(INFINITY);
-    const bool ok = (l[0] > T(0)) && (l[4] > T(0)) && (l[0] < inf) && (l[4] < inf) &&
-                    (r[0] > T(0)) && (r[4] > T(0)) && (r[0] < inf) && (r[4] < inf);
+    const T l0 = lc[0] + T(0.5) * sl[0], l4 = lc[4] + T(0.5) * sl[4];
+    const T r0 = rc[0] - T(0.5) * sr[0], r4 = rc[4] - T(0.5) * sr[4];
+    const bool ok = (l0 > T(0)) && (l4 > T(0)) && (l0 < inf) && (l4 < inf) && (r0 > T(0)) &&
+                    (r4 > T(0)) && (r0 < inf) && (r4 < inf);
+    const T h = ok ? T(0.5) : T(0);
+    T l[9], r[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        l[q] = ok ? l[q] : lc[q];
-        r[q] = ok ? r[q] : rc[q];
+        l[q] = lc[comp[q]] + h * sl[comp[q]];
+        r[q] = rc[comp[q]] - h * sr[comp[q]];
     }
     const PrimN<T> WL{l[0], l[1], l[2], l[3], l[4], l[5], l[6], l[7], l[8]};
     const PrimN<T> WR{r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]};
     const FluxN<T> f = hll_flux(WL, WR, gamma, inv_gm1, c_h);
     out[0] = f.rho;
-    out[1] = ydir ? f.mt : f.mn;
-    out[2] = ydir ? f.mn : f.mt;
+    out[1] = YDIR ? f.mt : f.mn;
+    out[2] = YDIR ? f.mn : f.mt;
     out[3] = f.mz;
     out[4] = f.e;
-    out[5] = ydir ? f.bt : f.bn;
-    out[6] = ydir ? f.bn : f.bt;
+    out[5] = YDIR ? f.bt : f.bn;
+    out[6] = YDIR ? f.bn : f.bt;
     out[7] = f.bz;
     out[8] = f.psi;
+}
+
+// The same from the shared-memory tile: centres sW[c * nh + wl|wr], slopes sS[c * sn + il|ir].
+template <class T, bool YDIR>
+__device__ __forceinline__ void face_flux(const T* __restrict__ sS, int sn, int il, int ir,
+                                          const T* __restrict__ sW, int nh, int wl, int wr,
+                                          T gamma, T inv_gm1, T c_h, T (&out)[9])
+{
+    T lc[9], rc[9], sl[9], sr[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        lc[c] = sW[c * nh + wl];
+        rc[c] = sW[c * nh + wr];
+        sl[c] = sS[c * sn + il];
+        sr[c] = sS[c * sn + ir];
+    }
+    face_flux_regs<T, YDIR>(lc, sl, rc, sr, gamma, inv_gm1, c_h, out);
 }
 
 // One face of a sweep: flux (HLL + GLM + non-ideal E) into sF[c * fn + t]; sS/sn are the
@@ -150,7 +166,7 @@ __device__ __forceinline__ void face_item(const T* __restrict__ sW, const T* __r
     const int wr = (fy + 2) * HX + (fx + 2);
     const int wl = wr - (YDIR ? HX : 1);
     T out[9];
-    face_flux(sS, sn, il, ir, sW, S::NH, wl, wr, YDIR, gamma, inv_gm1, c_h, out);
+    face_flux<T, YDIR>(sS, sn, il, ir, sW, S::NH, wl, wr, gamma, inv_gm1, c_h, out);
     if constexpr (NI) {
         // Face-averaged J and B, E from Ohm's law (include/mhd/rhs.hpp:75-114).
         const int jr = (fy + 1) * S::JX + (fx + 1);

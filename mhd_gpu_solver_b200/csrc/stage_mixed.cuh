@@ -109,7 +109,6 @@ struct PolicyMixed {
     struct Raw {
         float v[9];
     };
-
     // Full-precision value of the stage input at (x, y): hi + lo.
     template <int STAGE, bool MASK>
     static __device__ __forceinline__ void full(const Args& a, const Geometry& g, int x, int y,
@@ -208,17 +207,36 @@ struct PolicyMixed {
             }
             return;
         }
-        const float* __restrict__ ih = a.uin.hi;
-        const float* __restrict__ il = a.uin.lo;
-        float* __restrict__ oh = a.out.hi;
-        float* __restrict__ ol = a.out.lo;
-        // every load before any store
+        const float* __restrict__ ih = a.uin.hi + o;
+        const float* __restrict__ il = a.uin.lo + o;
+        const float* __restrict__ oh = a.out.hi + o;
+        const float* __restrict__ ol = a.out.lo + o;
+        const size_t pl = g.plane;
+        update_ops<STAGE>(a, g, gx, gy, solid, L, dt, k, smax, [&](int i) {
+            const size_t q = static_cast<size_t>(i % 9) * pl;
+            return i < 9 ? __ldg(ih + q) : (i < 18 ? __ldg(il + q) : (i < 27 ? oh[q] : ol[q]));
+        });
+    }
+
+    // The stage update of one cell from its own-cell operands op(i): plane i % 9 of the input hi
+    // (i < 9) and lo (i < 18) planes and, in stage 2, of the U^n hi (i < 27) and lo (i < 36)
+    // planes, which the stage overwrites; all are read before any store.
+    template <int STAGE, class Op>
+    static __device__ __forceinline__ void update_ops(const Args& a, const Geometry& g, int gx,
+                                                      int gy, bool solid, const float (&L)[9],
+                                                      double dt, const Consts& k, double& smax,
+                                                      const Op& op)
+    {
+        const float dtf = static_cast<float>(dt);
+        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
+        float* __restrict__ oh = a.out.hi + o;
+        float* __restrict__ ol = a.out.lo + o;
+        const size_t pl = g.plane;
         float xh[9], xl[9];
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
-            const size_t q = static_cast<size_t>(c) * g.plane + o;
-            xh[c] = __ldg(ih + q);
-            xl[c] = __ldg(il + q);
+            xh[c] = op(c);
+            xl[c] = op(9 + c);
         }
         if constexpr (STAGE == 1) {
             // U* = U^n + dt L
@@ -227,18 +245,16 @@ struct PolicyMixed {
                 float s, e, h, l;
                 two_sum(xh[c], __fmul_rn(dtf, L[c]), s, e); // product rounded first: exact two-sum
                 fast_two_sum(s, xl[c] + e, h, l);
-                const size_t q = static_cast<size_t>(c) * g.plane + o;
-                oh[q] = h;
-                ol[q] = l;
+                oh[c * pl] = h;
+                ol[c * pl] = l;
             }
         } else {
             // U^{n+1} = (U^n + U*)/2 + (dt/2) L, U^n read from the output buffer (own cell)
             float nh[9], nl[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
-                const size_t q = static_cast<size_t>(c) * g.plane + o;
-                nh[c] = oh[q];
-                nl[c] = ol[q];
+                nh[c] = op(18 + c);
+                nl[c] = op(27 + c);
             }
             float rf[9];
 #pragma unroll
@@ -249,9 +265,8 @@ struct PolicyMixed {
                 // halving is exact; then add the increment
                 two_sum(0.5f * h, __fmul_rn(0.5f * dtf, L[c]), s, e);
                 fast_two_sum(s, 0.5f * l + e, h, l);
-                const size_t q = static_cast<size_t>(c) * g.plane + o;
-                oh[q] = h;
-                ol[q] = l;
+                oh[c * pl] = h;
+                ol[c * pl] = l;
                 rf[c] = h;
             }
             if (!solid) {

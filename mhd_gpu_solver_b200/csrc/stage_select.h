@@ -1,8 +1,9 @@
 // Host-side table of the compiled stage-kernel instantiations. Each precision form is compiled
-// in its own translation unit (kernels_f64.cu, kernels_mixed.cu) for a few tile configurations;
-// configuration 0 is the default and the only one instantiated for every combination of limiter,
-// non-ideal terms and mask. The other configurations exist for the ideal, unmasked case and are
-// chosen by the autotuner (mhdb_autotune) per grid size class.
+// in its own translation unit (kernels_f64.cu, kernels_mixed.cu) for a few configurations of the
+// shared-memory tile kernel (stage_kernel.cuh) and of the warp strip-march kernel
+// (march_kernel.cuh); configuration 0 is the default tile kernel and the only one instantiated
+// for every combination of limiter, non-ideal terms and mask. The other configurations exist for
+// the ideal, unmasked case and are chosen by the autotuner per grid size class.
 #pragma once
 
 #include <cstddef>
@@ -18,12 +19,16 @@ using StageFnMx = void (*)(StageArgsMx);
 struct StageKernels {
     StageFnF64 f64_stage1 = nullptr, f64_stage2 = nullptr;
     StageFnMx mx_stage1 = nullptr, mx_stage2 = nullptr;
-    int tile_x = 0, tile_y = 0, threads = 0;
-    size_t smem = 0; // 0: no such configuration
+    int tile_x = 0, tile_y = 0, threads = 0; // threads == 0: no such configuration
+    size_t smem = 0, smem2 = 0;               // dynamic shared memory per block, stage 1 and 2
 };
 
+enum StageKernelKind : int { kKindTile = 0, kKindTileMerged = 1, kKindMarch = 2 };
+
+// tile_x x tile_y: interior cells one block covers (strip march: warps x 28 columns by the rows
+// of a warp's segment).
 struct TileConfigInfo {
-    int tile_x, tile_y, threads, min_blocks, merged;
+    int tile_x, tile_y, threads, min_blocks, kind;
 };
 
 // Number of tile configurations compiled per precision form, and their shapes.
@@ -33,7 +38,7 @@ TileConfigInfo stage_config_info_f64(int config);
 TileConfigInfo stage_config_info_mixed(int config);
 
 // Kernels of one configuration; config != 0 is available only for ideal, unmasked solves
-// (smem == 0 otherwise).
+// (threads == 0 otherwise).
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);
 

@@ -296,3 +296,40 @@ def test_every_tile_configuration_matches_oracle(precision):
         assert r.steps == sr
         err = rel_l1(got, ref)
         assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (cfg, err)
+
+
+MARCH_CASES = [
+    # nx, ny, bc_x, bc_y, state, limiter: partial strips (28 columns per warp) and partial row
+    # segments, every boundary rule combination, every limiter, smooth and shocked states
+    (61, 150, orc.PERIODIC, orc.PERIODIC, "fourier", orc.VANLEER),
+    (61, 150, orc.OUTFLOW, orc.OUTFLOW, "quadrants", orc.MC),
+    (29, 33, orc.OUTFLOW, orc.PERIODIC, "fourier", orc.MINMOD),
+    (140, 70, orc.PERIODIC, orc.OUTFLOW, "quadrants", orc.VANLEER),
+    (5, 7, orc.PERIODIC, orc.PERIODIC, "fourier", orc.MC),
+]
+
+
+@pytest.mark.parametrize("precision", [_capi.FP64, _capi.FP32])
+@pytest.mark.parametrize("case", range(len(MARCH_CASES)))
+def test_strip_march_configurations_match_oracle(precision, case):
+    nx, ny, bcx, bcy, state, lim = MARCH_CASES[case]
+    bc = (bcx, bcy)
+    prim = (wl.fourier_state(nx, ny, 9) if state == "fourier" else wl.four_quadrant(nx, ny, 3))
+    U0 = initial_state(prim, 5.0 / 3.0, bc)
+    p = orc.Params(limiter=lim, max_steps=25, fixed_steps=True)
+    ref, tr, sr, _ = orc.solve(U0, orc.Grid(nx, ny), p, bc)
+    tol = FP64_L1 if precision == _capi.FP64 else MIXED_L1
+    marches = [c for c in _capi.tile_configs(precision) if c["kind"].startswith("march")]
+    assert marches
+    for cfg in marches:
+        dev = _capi.DeviceSolver(nx, ny, precision=precision)
+        dev.set_tile_config(cfg["config"])
+        dev.configure(bcx, bcy)
+        dev.upload(U0)
+        r = dev.solve_steps(_capi.make_params(limiter=lim), 25)
+        got = dev.download()
+        dev.close()
+        assert r.steps == sr
+        assert abs(r.t - tr) <= (1e-12 if precision == _capi.FP64 else 1e-6) * max(1.0, tr)
+        err = rel_l1(got, ref)
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (cfg, err)
