@@ -160,9 +160,11 @@ long long mhdb_launch_count(const mhdb_solver* h);
    the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells
    one CTA covers (tile width and height), threads per CTA and the minimum CTAs per SM of one
    configuration; mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile,
-   separate x and y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps) or MHDB_KERNEL_MARCH (warp
-   strip march, 28 columns per warp), or -1 for an unknown configuration. */
-enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2 };
+   separate x and y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp
+   strip march, 28 columns per warp) or MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk
+   copies into shared memory; FP32-mixed only), or -1 for an unknown configuration. */
+enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,
+       MHDB_KERNEL_MARCH_TMA = 3 };
 int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);

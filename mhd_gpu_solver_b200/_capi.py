@@ -268,7 +268,7 @@ class DeviceSolver:
         raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
 
 
-KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march"}
+KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma"}
 
 
 def tile_configs(precision: int) -> list[dict]:

@@ -4,6 +4,7 @@
 #include <type_traits>
 
 #include "march_kernel.cuh"
+#include "march_tma.cuh"
 #include "stage_kernel.cuh"
 #include "stage_select.h"
 
@@ -42,6 +43,20 @@ struct MarchCfg {
     static constexpr bool MARCH = true;
 };
 
+// TMA-fed strip-march configuration (FP32-mixed form only): NW warps per block, LY rows per
+// warp, MINB blocks per SM.
+template <int NW_, int LY_, int MINB_, bool HF_ = true>
+struct MarchTmaCfg {
+    static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
+    static constexpr bool HF = HF_; // wait for the halo row before the x sweep
+    static constexpr bool MARCH_TMA = true;
+};
+
+template <class Cfg, class = void>
+struct is_march_tma : std::false_type {};
+template <class Cfg>
+struct is_march_tma<Cfg, std::void_t<decltype(Cfg::MARCH_TMA)>> : std::true_type {};
+
 template <class Cfg, class = void>
 struct is_march : std::false_type {};
 template <class Cfg>
@@ -50,7 +65,18 @@ struct is_march<Cfg, std::void_t<decltype(Cfg::MARCH)>> : std::true_type {};
 template <class Policy, class Cfg, int L, bool NI, bool MASK>
 void fill_pair(StageKernels& k)
 {
-    if constexpr (is_march<Cfg>::value) {
+    if constexpr (is_march_tma<Cfg>::value) {
+        static_assert(!NI && !MASK, "the strip-march kernel serves ideal, unmasked solves");
+        static_assert(sizeof(typename Policy::T) == 4, "the TMA strip march is FP32-mixed only");
+        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF>;
+        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF>;
+        k.tile_x = Cfg::NW * kMarchOwned;
+        k.tile_y = Cfg::LY;
+        k.threads = Cfg::NW * 32;
+        k.smem = march_tma_smem_bytes<1>(Cfg::NW);
+        k.smem2 = march_tma_smem_bytes<2>(Cfg::NW);
+        return;
+    } else if constexpr (is_march<Cfg>::value) {
         static_assert(!NI && !MASK, "the strip-march kernel serves ideal, unmasked solves");
         using T = typename Policy::T;
         auto s1 = march_kernel<Policy, L, 1, Cfg::LY, Cfg::NW, Cfg::MINB>;

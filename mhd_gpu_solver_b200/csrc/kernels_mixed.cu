@@ -14,12 +14,18 @@ using Cfg6 = MarchCfg<4, 64, 4>;
 using Cfg7 = MarchCfg<4, 32, 4>;
 using Cfg8 = MarchCfg<4, 128, 4>;
 using Cfg9 = MarchCfg<4, 64, 3>;
+using Cfg10 = MarchTmaCfg<4, 32, 4>;
+using Cfg11 = MarchTmaCfg<4, 32, 5>;
+using Cfg12 = MarchTmaCfg<4, 64, 5>;
+using Cfg13 = MarchTmaCfg<4, 32, 4, false>;
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
     {32, 16, 256, 2, kKindTileMerged}, {32, 8, 320, 3, kKindTileMerged},
     {112, 64, 128, 4, kKindMarch},     {112, 32, 128, 4, kKindMarch},
-    {112, 128, 128, 4, kKindMarch},    {112, 64, 128, 3, kKindMarch}};
+    {112, 128, 128, 4, kKindMarch},    {112, 64, 128, 3, kKindMarch},
+    {112, 32, 128, 4, kKindMarchTma},  {112, 32, 128, 5, kKindMarchTma},
+    {112, 64, 128, 5, kKindMarchTma},  {112, 32, 128, 4, kKindMarchTma}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -48,6 +54,14 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_ideal<PolicyMixed, Cfg8>(limiter, nonideal, mask);
     case 9:
         return select_ideal<PolicyMixed, Cfg9>(limiter, nonideal, mask);
+    case 10:
+        return select_ideal<PolicyMixed, Cfg10>(limiter, nonideal, mask);
+    case 11:
+        return select_ideal<PolicyMixed, Cfg11>(limiter, nonideal, mask);
+    case 12:
+        return select_ideal<PolicyMixed, Cfg12>(limiter, nonideal, mask);
+    case 13:
+        return select_ideal<PolicyMixed, Cfg13>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

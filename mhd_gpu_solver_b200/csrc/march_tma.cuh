@@ -1,0 +1,287 @@
+// TMA-fed warp strip-march stage kernel of the FP32-mixed form (ideal GLM-MHD, no solid mask).
+//
+// The arithmetic is that of march_kernel.cuh (register-resident stencil, shuffle x sweep, every
+// slope limited once and every face evaluated once), so both kernels produce the same values.
+// What changes is how rows reach the warp: each warp runs a two-slot TMA pipeline per stream of
+// rows, driven by lane 0 and completed on mbarriers:
+//   * halo stream: the stage input's 9 hi planes of row y + 2, columns x0 - 4 .. x0 + 31
+//     (box 36 x 1 x 9; the x origin x0 - 4 is a multiple of 4 floats, 16 bytes), issued two
+//     rows ahead of its use; lane l reads column x0 - 2 + l at offset l + 2;
+//   * own stream: the hi and lo planes of row y, owned columns x0 .. x0 + 27 (box 28 x 1 x 18),
+//     of the stage input and, in stage 2, of U^n (updated in place), issued two rows ahead.
+// Rows are addressed through the boundary map (periodic wrap / outflow clamp in y), so the
+// copies never leave the interior in y. Lanes whose column lies outside [0, nx) (x halo of the
+// first and last strips) load their values directly through the x map instead of from the box.
+// Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records kStatusWaitTimeout in
+// the Ctrl block, waits (bounded) for its copies still in flight and stops its strip.
+#pragma once
+
+#include "march_kernel.cuh"
+#include "stage_mixed.cuh"
+#include "tma.cuh"
+
+namespace mhdb {
+
+template <int STAGE>
+struct MarchTmaLayout {
+    static constexpr int kHaloFloats = 9 * kTmaHaloW;             // 324 floats, 1296 B
+    static constexpr int kHaloBytes = kHaloFloats * 4;
+    static constexpr int kHaloSlot = (kHaloBytes + 127) / 128 * 128; // 1408 B
+    static constexpr int kOwnBoxBytes = 18 * kTmaOwnW * 4;          // 2016 B per box
+    static constexpr int kOwnBoxSlot = (kOwnBoxBytes + 127) / 128 * 128; // 2048 B
+    static constexpr int kOwnBoxes = STAGE == 1 ? 1 : 2;
+    static constexpr int kOwnSlot = kOwnBoxes * kOwnBoxSlot;
+    static constexpr int kOwnTx = kOwnBoxes * kOwnBoxBytes;       // transaction bytes per row
+    static constexpr int kBarOff = 2 * kHaloSlot + 2 * kOwnSlot;
+    static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
+};
+
+template <int STAGE>
+constexpr size_t march_tma_smem_bytes(int warps)
+{
+    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE>::kWarpBytes + 128;
+}
+
+template <int L, int STAGE, int LY, bool HF>
+__device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
+                                                  int x0, int y0, int lane, unsigned char* wbase)
+{
+    using Policy = PolicyMixed;
+    using T = float;
+    using Raw = Policy::Raw;
+    using Lay = MarchTmaLayout<STAGE>;
+    constexpr unsigned kFull = 0xffffffffu;
+    const Geometry& g = a.geom;
+    const Consts& k = a.k;
+    const double dt = a.ctrl->dt;
+    const double c_h64 = a.ctrl->c_h;
+    const T c_h = static_cast<T>(c_h64);
+    const T gamma = static_cast<T>(k.gamma);
+    const T inv_gm1 = static_cast<T>(k.inv_gm1);
+    const T inv_dx = static_cast<T>(k.inv_dx), inv_dy = static_cast<T>(k.inv_dy);
+    const double psi_damp = (c_h64 > 0.0 && k.glm_alpha > 0.0) ? (c_h64 * k.glm_alpha / k.h) : 0.0;
+
+    const int gx = x0 - 2 + lane;
+    const int sx = map_index(gx, g.nx, g.bc_x);
+    const bool in_x = gx >= 0 && gx < g.nx;
+    const bool own = lane >= 2 && lane < 2 + kMarchOwned && gx < g.nx;
+    const int y1 = min(y0 + LY, g.ny);
+    const int nrows = y1 - y0;
+
+    const float* halo_f = reinterpret_cast<const float*>(wbase);
+    const float* own_f = reinterpret_cast<const float*>(wbase + 2 * Lay::kHaloSlot);
+    const uint32_t halo_s = smem_addr(wbase);
+    const uint32_t own_s = halo_s + 2 * Lay::kHaloSlot;
+    const uint32_t bar_s = halo_s + Lay::kBarOff; // halo: +0, +8; own: +16, +24
+
+    if (lane == 0) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            mbar_init(bar_s + 8 * b, 1);
+        }
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    // Item i of the halo stream is row y0 + 2 + i; item i of the own stream is row y0 + i; both
+    // use slot i & 1, whose (i >> 1)-th phase completes it.
+    auto issue_halo = [&](int i) {
+        const uint32_t slot = static_cast<uint32_t>(i & 1);
+        const uint32_t bar = bar_s + 8 * slot;
+        mbar_arrive_expect_tx(bar, Lay::kHaloBytes);
+        tma_load_3d(halo_s + slot * Lay::kHaloSlot, &m.in_halo, bar, x0 - 4,
+                    map_index(y0 + 2 + i, g.ny, g.bc_y), 0);
+    };
+    auto issue_own = [&](int i) {
+        const uint32_t slot = static_cast<uint32_t>(i & 1);
+        const uint32_t bar = bar_s + 16 + 8 * slot;
+        const uint32_t dst = own_s + slot * Lay::kOwnSlot;
+        mbar_arrive_expect_tx(bar, Lay::kOwnTx);
+        tma_load_3d(dst, &m.in_own, bar, x0, y0 + i, 0);
+        if constexpr (STAGE == 2) {
+            tma_load_3d(dst + Lay::kOwnBoxSlot, &m.out_own, bar, x0, y0 + i, 0);
+        }
+    };
+    int halo_issued = 0, own_issued = 0, halo_done = 0, own_done = 0;
+    if (lane == 0) {
+        issue_halo(0);
+        issue_own(0);
+        if (nrows > 1) {
+            issue_halo(1);
+            issue_own(1);
+        }
+    }
+    halo_issued = own_issued = nrows > 1 ? 2 : 1;
+
+    auto load = [&](int y, Raw& r) { Policy::load_raw(a, g, sx, map_index(y, g.ny, g.bc_y), r); };
+    auto prim = [&](int y, const Raw& r, T (&w)[9]) {
+        Policy::template raw_prim<STAGE, false>(a, g, sx, map_index(y, g.ny, g.bc_y), r, k, w);
+    };
+
+    // Prologue (direct loads): rows y0-2 .. y0+1, slopes of rows y0-1 and y0, flux G(y0 - 1/2).
+    T Wm[9], Wp[9], sYc[9], Gm[9];
+    {
+        Raw r0, r1, r2, r3;
+        load(y0 - 2, r0);
+        load(y0 - 1, r1);
+        load(y0, r2);
+        load(y0 + 1, r3);
+        T wa[9], wb[9], sYm[9];
+        prim(y0 - 2, r0, wa);
+        prim(y0 - 1, r1, wb);
+        prim(y0, r2, Wm);
+        prim(y0 + 1, r3, Wp);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            sYm[c] = limit_half_slope<L>(wb[c] - wa[c], Wm[c] - wb[c]);
+            sYc[c] = limit_half_slope<L>(Wm[c] - wb[c], Wp[c] - Wm[c]);
+        }
+        face_flux_regs<T, true, true>(wb, sYm, Wm, sYc, gamma, inv_gm1, c_h, Gm);
+    }
+
+    double smax = 0.0;
+    bool failed = false;
+#pragma unroll 1
+    for (int i = 0; i < nrows; ++i) {
+        const int y = y0 + i;
+        // x sweep of row y: dF = F(x + 1/2) - F(x - 1/2) on the owned lanes
+        T dF[9];
+        auto x_sweep = [&]() {
+            T Wn[9], sX[9], sXn[9], F[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                Wn[c] = __shfl_down_sync(kFull, Wm[c], 1);
+                const T dR = Wn[c] - Wm[c];
+                const T dL = __shfl_up_sync(kFull, dR, 1);
+                sX[c] = limit_half_slope<L>(dL, dR);
+            }
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                sXn[c] = __shfl_down_sync(kFull, sX[c], 1);
+            }
+            face_flux_regs<T, false, true>(Wm, sX, Wn, sXn, gamma, inv_gm1, c_h, F);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                dF[c] = F[c] - __shfl_up_sync(kFull, F[c], 1);
+            }
+        };
+        if constexpr (!HF) {
+            x_sweep();
+        }
+        // row y + 2 from the halo stream
+        Raw rn;
+        {
+            const uint32_t slot = static_cast<uint32_t>(i & 1);
+            const bool ok = mbar_wait(bar_s + 8 * slot, static_cast<uint32_t>((i >> 1) & 1));
+            if (__any_sync(kFull, !ok)) {
+                failed = true;
+                break;
+            }
+            halo_done = i + 1;
+            if (in_x) {
+                const float* src = halo_f + slot * (Lay::kHaloSlot / 4) + lane + 2;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    rn.v[c] = src[c * kTmaHaloW];
+                }
+            } else {
+                load(y + 2, rn);
+            }
+            __syncwarp();
+            if (i + 2 < nrows) {
+                if (lane == 0) {
+                    issue_halo(i + 2);
+                }
+                halo_issued = i + 3;
+            }
+        }
+        T W2[9], sYn[9], Gp[9];
+        prim(y + 2, rn, W2);
+        if constexpr (HF) {
+            x_sweep(); // after the halo wait: the x and y fluxes share one scheduling region
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            sYn[c] = limit_half_slope<L>(Wp[c] - Wm[c], W2[c] - Wp[c]);
+        }
+        face_flux_regs<T, true, true>(Wm, sYc, Wp, sYn, gamma, inv_gm1, c_h, Gp);
+        // own-cell operands of row y from the own stream, then the stage update
+        {
+            const uint32_t slot = static_cast<uint32_t>(i & 1);
+            const bool ok = mbar_wait(bar_s + 16 + 8 * slot, static_cast<uint32_t>((i >> 1) & 1));
+            if (__any_sync(kFull, !ok)) {
+                failed = true;
+                break;
+            }
+            own_done = i + 1;
+            if (own) {
+                T Lc[9];
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    Lc[c] = -dF[c] * inv_dx - (Gp[c] - Gm[c]) * inv_dy; // include/mhd/rhs.hpp:121
+                }
+                if (psi_damp != 0.0) {
+                    Lc[8] -= static_cast<float>(psi_damp) * Wm[8]; // include/mhd/rhs.hpp:219-225
+                }
+                const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
+                Policy::template update_ops<STAGE>(a, g, gx, y, false, Lc, dt, k, smax, [&](int q) {
+                    return q < 18 ? src[q * kTmaOwnW]
+                                  : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
+                });
+            }
+            __syncwarp();
+            if (i + 2 < nrows) {
+                if (lane == 0) {
+                    issue_own(i + 2);
+                }
+                own_issued = i + 3;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            Wm[c] = Wp[c];
+            Wp[c] = W2[c];
+            sYc[c] = sYn[c];
+            Gm[c] = Gp[c];
+        }
+    }
+    if (failed) {
+        // Record the failure and let every copy of this warp land before the CTA can exit.
+        if (lane == 0) {
+            atomicOr(&a.ctrl->status, static_cast<int>(kStatusWaitTimeout));
+        }
+        for (int j = halo_done; j < halo_issued; ++j) {
+            mbar_wait(bar_s + 8 * (j & 1), static_cast<uint32_t>((j >> 1) & 1));
+        }
+        for (int j = own_done; j < own_issued; ++j) {
+            mbar_wait(bar_s + 16 + 8 * (j & 1), static_cast<uint32_t>((j >> 1) & 1));
+        }
+        return 0.0;
+    }
+    return smax;
+}
+
+template <int L, int STAGE, int LY, int NW, int MINB, bool HF>
+__global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArgsMx a,
+                                                                   const __grid_constant__ MarchTmaMaps m)
+{
+    if (a.ctrl->finished != 0) {
+        return;
+    }
+    extern __shared__ unsigned char march_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // 128-byte aligned start, derived from the shared array itself so that every access through
+    // it compiles to a shared-memory load
+    unsigned char* base = march_smem + ((128u - (smem_addr(march_smem) & 127u)) & 127u);
+    const int x0 = (blockIdx.x * NW + warp) * kMarchOwned;
+    double smax = 0.0;
+    if (x0 < a.geom.nx) { // warp-uniform
+        smax = march_tma_strip<L, STAGE, LY, HF>(a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
+                                             base + warp * MarchTmaLayout<STAGE>::kWarpBytes);
+    }
+    if constexpr (STAGE == 2) {
+        reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
+    }
+}
+
+} // namespace mhdb

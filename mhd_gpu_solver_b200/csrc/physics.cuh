@@ -129,6 +129,25 @@ __device__ __forceinline__ T limit_slope(T a, T b)
     }
 }
 
+// Half of the limited slope, lim(a, b) / 2, computed directly (halving is exact, so this is the
+// same value as 0.5 * limit_slope): van Leer ab / (a + b), MC minmod((a + b) / 4, minmod(a, b)),
+// minmod minmod(a / 2, b / 2).
+template <int L, class T>
+__device__ __forceinline__ T limit_half_slope(T a, T b)
+{
+    if constexpr (L == kMinmod) {
+        return minmod(T(0.5) * a, T(0.5) * b);
+    } else if constexpr (L == kMC) {
+        return minmod(T(0.25) * (a + b), minmod(a, b));
+    } else if constexpr (sizeof(T) == 4) {
+        const float p = a * b;
+        const float q = p * fast_rcp(a + b);
+        return (p <= 0.0f) ? 0.0f : q;
+    } else {
+        return (a * b <= T(0)) ? T(0) : (a * b) / (a + b);
+    }
+}
+
 // Face i-1/2 from cells (i-2, i-1, i, i+1); include/mhd/kernels/muscl_hll.hpp:59-68.
 template <int L, class T>
 __device__ __forceinline__ void reconstruct(T wmm, T wm, T w0, T wp, T& left, T& right)

@@ -92,8 +92,9 @@ __device__ __forceinline__ void face_states(const T* __restrict__ sW, T* __restr
 // One face flux from the centre values lc, rc and limited slopes sl, sr (physical component
 // order) of its two cells: left state W(l) + s(l)/2, right state W(r) - s(r)/2
 // (include/mhd/kernels/muscl_hll.hpp:66-67), with the both-sides first-order fallback of
-// muscl_hll.hpp:145-168. Output in physical component order.
-template <class T, bool YDIR>
+// muscl_hll.hpp:145-168. Output in physical component order. HALF: sl and sr hold half slopes
+// s/2 (exact halves), so the face states are W(l) + s'(l) and W(r) - s'(r), the same values.
+template <class T, bool YDIR, bool HALF = false>
 __device__ __forceinline__ void face_flux_regs(const T (&lc)[9], const T (&sl)[9],
                                                const T (&rc)[9], const T (&sr)[9], T gamma,
                                                T inv_gm1, T c_h, T (&out)[9])
@@ -104,11 +105,12 @@ __device__ __forceinline__ void face_flux_regs(const T (&lc)[9], const T (&sl)[9
     // W + h s with h = 1/2 (second order) or h = 0 (first order: W + 0 s = W exactly for finite
     // slopes, and 0.5 s is exact, so both cases give the reference's values).
     const T inf = T(INFINITY);
-    const T l0 = lc[0] + T(0.5) * sl[0], l4 = lc[4] + T(0.5) * sl[4];
-    const T r0 = rc[0] - T(0.5) * sr[0], r4 = rc[4] - T(0.5) * sr[4];
+    const T hs = HALF ? T(1) : T(0.5);
+    const T l0 = lc[0] + hs * sl[0], l4 = lc[4] + hs * sl[4];
+    const T r0 = rc[0] - hs * sr[0], r4 = rc[4] - hs * sr[4];
     const bool ok = (l0 > T(0)) && (l4 > T(0)) && (l0 < inf) && (l4 < inf) && (r0 > T(0)) &&
                     (r4 > T(0)) && (r0 < inf) && (r4 < inf);
-    const T h = ok ? T(0.5) : T(0);
+    const T h = ok ? hs : T(0);
     T l[9], r[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {

@@ -2,9 +2,10 @@
 // with |lo| <= ulp(hi)/2 (~48 significant bits). Precision rules:
 //   * reconstruction, HLL fluxes, non-ideal terms and the divergence run in FP32 on hi;
 //   * the stage updates U* = U^n + dt L (include/mhd/field_ops.hpp:51) and
-//     U^{n+1} = (U^n + U*)/2 + (dt/2) L (field_ops.hpp:61) are done in double-FP32 arithmetic on
-//     the (hi, lo) pairs with error-free two-sums, so the RK2 combination loses no bits of the
-//     state (only the FP32 increment dt L carries FP32 rounding);
+//     U^{n+1} = (U^n + U*)/2 + (dt/2) L (field_ops.hpp:61) add an FP32 stage increment (dt L,
+//     resp. (U* - U^n)/2 + (dt/2) L) to the (hi, lo) pair of U^n with error-free two-sums, so
+//     the RK2 combination loses no bits of the state (only the increment carries FP32 rounding,
+//     relative to its own size);
 //   * pressure recovery p = (gamma-1)(E - rho v^2/2 - B^2/2) is redone in FP64 from hi + lo in
 //     cells where the FP32 subtraction cancels (p/(gamma-1) < E / kCancelRatio: low beta or high
 //     Mach) or is not finite;
@@ -249,22 +250,26 @@ struct PolicyMixed {
                 ol[c * pl] = l;
             }
         } else {
-            // U^{n+1} = (U^n + U*)/2 + (dt/2) L, U^n read from the output buffer (own cell)
+            // U^{n+1} = (U^n + U*)/2 + (dt/2) L = U^n + d with d = (U* - U^n)/2 + (dt/2) L,
+            // U^n read from the output buffer (own cell). d is a stage increment: it is formed
+            // in FP32 (its rounding is relative to d, like that of dt L in stage 1) and added to
+            // the (hi, lo) pair of U^n exactly.
             float nh[9], nl[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 nh[c] = op(18 + c);
                 nl[c] = op(27 + c);
             }
+            const float half_dt = 0.5f * dtf;
             float rf[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 float s, e, h, l;
-                two_sum(nh[c], xh[c], s, e);
-                fast_two_sum(s, (nl[c] + xl[c]) + e, h, l);
-                // halving is exact; then add the increment
-                two_sum(0.5f * h, __fmul_rn(0.5f * dtf, L[c]), s, e);
-                fast_two_sum(s, 0.5f * l + e, h, l);
+                const float d = __fmaf_rn(half_dt, L[c],
+                                          __fmul_rn(0.5f, __fadd_rn(__fsub_rn(xh[c], nh[c]),
+                                                                    __fsub_rn(xl[c], nl[c]))));
+                two_sum(nh[c], d, s, e);
+                fast_two_sum(s, nl[c] + e, h, l);
                 oh[c * pl] = h;
                 ol[c * pl] = l;
                 rf[c] = h;

@@ -10,20 +10,23 @@
 
 #include "stage_f64.cuh"
 #include "stage_mixed.cuh"
+#include "tma.cuh"
 
 namespace mhdb {
 
 using StageFnF64 = void (*)(StageArgsF64);
 using StageFnMx = void (*)(StageArgsMx);
+using StageFnMxTma = void (*)(StageArgsMx, MarchTmaMaps); // TMA-fed kernels take tensor maps
 
 struct StageKernels {
     StageFnF64 f64_stage1 = nullptr, f64_stage2 = nullptr;
     StageFnMx mx_stage1 = nullptr, mx_stage2 = nullptr;
+    StageFnMxTma mx_tma1 = nullptr, mx_tma2 = nullptr;
     int tile_x = 0, tile_y = 0, threads = 0; // threads == 0: no such configuration
     size_t smem = 0, smem2 = 0;               // dynamic shared memory per block, stage 1 and 2
 };
 
-enum StageKernelKind : int { kKindTile = 0, kKindTileMerged = 1, kKindMarch = 2 };
+enum StageKernelKind : int { kKindTile = 0, kKindTileMerged = 1, kKindMarch = 2, kKindMarchTma = 3 };
 
 // tile_x x tile_y: interior cells one block covers (strip march: warps x 28 columns by the rows
 // of a warp's segment).

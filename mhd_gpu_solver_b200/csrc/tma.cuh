@@ -1,0 +1,103 @@
+// Tensor-memory-accelerator (TMA) bulk copies into shared memory, completed on mbarriers.
+//
+// Only tiled, non-multicast loads of this GPU's own memory are issued (cp.async.bulk.tensor
+// .3d.shared::cluster.global.mbarrier::complete_tx::bytes; a CTA launched without a cluster is a
+// cluster of one). Every wait is bounded: mbar_wait gives up after kWaitNs of global-timer time
+// and returns false, so a kernel can record the failure and drain its copies instead of spinning.
+#pragma once
+
+#include <cuda.h>
+#include <cstdint>
+
+namespace mhdb {
+
+// Tensor maps of one strip-march stage (stage_mixed.cuh state): 3D views (x, y, plane) of the
+// stage input and output buffers over the 18 float planes (9 hi, then 9 lo) of a mixed state.
+//   in_halo: stage input, box {kTmaHaloW, 1, 9}    (hi planes of one row, x halo included)
+//   in_own:  stage input, box {kTmaOwnW, 1, 18}    (hi and lo of a warp's owned columns)
+//   out_own: stage output, box {kTmaOwnW, 1, 18}   (stage 2 only: U^n, updated in place)
+struct MarchTmaMaps {
+    CUtensorMap in_halo;
+    CUtensorMap in_own;
+    CUtensorMap out_own;
+};
+
+constexpr int kTmaOwnW = 28;  // owned columns of a warp (a multiple of 4: 16-byte x offsets)
+constexpr int kTmaHaloW = 36; // columns x0 - 4 .. x0 + 31 (x0 - 4 is a multiple of 4)
+constexpr unsigned long long kWaitNs = 500000000ull; // 0.5 s per bounded wait
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Makes mbarrier initialisation visible to the async proxy (the TMA unit).
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the phase with the given parity to complete; false after kWaitNs without completion.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) {
+        return true;
+    }
+    const unsigned long long t0 = global_ns();
+#pragma unroll 1
+    while (true) {
+#pragma unroll 1
+        for (int i = 0; i < 64; ++i) {
+            if (mbar_try_wait(bar, parity)) {
+                return true;
+            }
+        }
+        if (global_ns() - t0 > kWaitNs) {
+            return false;
+        }
+    }
+}
+
+// 3D tiled load of one box at (x, y, z) of the tensor map into shared memory at dst; completion
+// is signalled on the mbarrier bar as transaction bytes.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+} // namespace mhdb
