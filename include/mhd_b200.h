@@ -156,8 +156,9 @@ int mhdb_profile_read(mhdb_solver* h, double* ms_stage1, int* n_stage1, double* 
 long long mhdb_launch_count(const mhdb_solver* h);
 
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the default) serves every
-   solve; the others exist for ideal solves without a mask and are picked per grid size class by
-   the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells
+   solve; the others serve solves without a mask (the strip-march ones ideal and non-ideal solves,
+   the other tile ones ideal solves only; a solve they do not serve runs configuration 0) and are
+   picked per grid size class by the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells
    one CTA covers (tile width and height), threads per CTA and the minimum CTAs per SM of one
    configuration; mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile,
    separate x and y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp
@@ -198,6 +199,13 @@ int mhdb_batch_add_generated(mhdb_batch* b, const mhdb_grid* grid, const mhdb_pa
 
 /* Advance every unfinished solve by up to nsteps steps; *active (optional) = unfinished count. */
 int mhdb_batch_step(mhdb_batch* b, int nsteps, int* active);
+
+/* mhdb_batch_step in two halves: mhdb_batch_launch issues the steps and returns without waiting;
+   mhdb_batch_poll waits for them and refreshes every solve's status (as mhdb_batch_step does at
+   its end). Between the two, solves that the previous poll reported finished can be downloaded
+   (mhdb_batch_download copies them beside the running steps) and removed. */
+int mhdb_batch_launch(mhdb_batch* b, int nsteps);
+int mhdb_batch_poll(mhdb_batch* b, int* active);
 
 /* t, steps, c_h and whether the solve has finished; MHDB_MAX_STEPS / MHDB_BAD_TIMESTEP as
    mhdb_solve would report them. */

@@ -30,6 +30,7 @@ EXPORTS = (
     "mhdb_batch_create", "mhdb_batch_destroy", "mhdb_batch_last_error", "mhdb_batch_add",
     "mhdb_batch_remove", "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download",
     "mhdb_batch_info", "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
+    "mhdb_batch_launch", "mhdb_batch_poll",
 )
 
 
@@ -111,6 +112,8 @@ def _load() -> C.CDLL:
                             C.c_size_t, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_remove": ([b, C.c_int], C.c_int),
         "mhdb_batch_step": ([b, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mhdb_batch_launch": ([b, C.c_int], C.c_int),
+        "mhdb_batch_poll": ([b, C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_status": ([b, C.c_int, C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_download": ([b, C.c_int, _PPD, C.c_size_t], C.c_int),
         "mhdb_batch_info": ([b, C.POINTER(C.c_size_t), C.POINTER(C.c_int),

@@ -5,8 +5,9 @@ CTA, minimum CTAs per SM; ``_capi.tile_configs``). For a grid size class (interi
 to a power of two, per precision form and limiter) the tuner times each configuration on a
 synthetic smooth state for a few RK2 steps, with CUDA events on the solver's stream, and
 remembers the fastest. Results are cached in memory for the process and can be saved to / loaded
-from a JSON file. Configurations other than 0 serve ideal, unmasked solves only; for other solves
-the runtime always uses configuration 0.
+from a JSON file. Configurations other than 0 serve unmasked solves (the strip-march ones ideal
+and non-ideal solves, the other tile ones ideal solves only); a solve that the chosen
+configuration does not serve runs configuration 0.
 """
 
 from __future__ import annotations

@@ -82,6 +82,16 @@ class BatchSolver:
         self._raise(_capi.lib.mhdb_batch_step(self._b, int(nsteps), C.byref(active)))
         return active.value
 
+    def launch(self, nsteps: int) -> None:
+        """Issue up to nsteps steps of every unfinished solve without waiting for them."""
+        self._raise(_capi.lib.mhdb_batch_launch(self._b, int(nsteps)))
+
+    def poll(self) -> int:
+        """Wait for the issued steps and refresh every status; returns the unfinished count."""
+        active = C.c_int()
+        self._raise(_capi.lib.mhdb_batch_poll(self._b, C.byref(active)))
+        return active.value
+
     def status(self, sid: int):
         """(Result, finished); raises for a solve that hit max_steps or a bad dt."""
         r = _capi.Result()

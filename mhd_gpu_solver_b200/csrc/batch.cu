@@ -3,8 +3,10 @@
 // A batch holds solves, each with its own grid, gamma, CFL, limiter, non-ideal coefficients,
 // boundary rule, time target and HBM-resident state (U^n and the stage state, stream-ordered
 // allocations). Every RK2 step is one persistent launch per stage and per (limiter, non-ideal)
-// combination present: each launch walks a tile work-list covering all unfinished solves of that
-// combination (batch_stage_kernel in stage_kernel.cuh). Each solve keeps its own Ctrl block (FP64
+// combination present: each launch walks a block work-list covering all unfinished solves of that
+// combination (FP64: the shared-memory tile kernel, batch_stage_kernel in stage_kernel.cuh;
+// FP32-mixed: the register strip march, batch_march_kernel in march_kernel.cuh). Each solve
+// keeps its own Ctrl block (FP64
 // clock, dt, c_h, step count) in one slot array, so one device-to-host copy reports every solve.
 // Chunks of steps are captured as CUDA graphs and replayed while the set of solves is unchanged.
 
@@ -185,13 +187,17 @@ struct BatchKernels<PolicyF64> {
     static size_t smem(bool ni) { return ni ? stage_smem_bytes<double, Cfg::TX, Cfg::TY, true>() : stage_smem_bytes<double, Cfg::TX, Cfg::TY, false>(); }
 };
 
+// FP32-mixed batches run the register strip march (4 warps x 28 columns by 32 rows per block).
 template <>
 struct BatchKernels<PolicyMixed> {
-    using Cfg = TileCfg<32, 16, 256, 3>;
+    struct Cfg {
+        static constexpr int NW = 4, LY = 32, MINB = 4;
+        static constexpr int TX = NW * kMarchOwned, TY = LY, NT = NW * 32;
+    };
     using Fn = void (*)(const BatchSolve<PolicyMixed>*, const int2*, int);
     template <int L, bool NI, int STAGE>
-    static Fn fn() { return batch_stage_kernel<PolicyMixed, L, NI, STAGE, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>; }
-    static size_t smem(bool ni) { return ni ? stage_smem_bytes<float, Cfg::TX, Cfg::TY, true>() : stage_smem_bytes<float, Cfg::TX, Cfg::TY, false>(); }
+    static Fn fn() { return batch_march_kernel<PolicyMixed, L, NI, STAGE, Cfg::LY, Cfg::NW, Cfg::MINB>; }
+    static size_t smem(bool) { return 0; }
 };
 
 template <class Policy>
@@ -234,6 +240,13 @@ struct mhdb_batch {
     int precision = MHDB_FP32;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // Downloads of finished solves run here, beside the steps in flight on `stream`.
+    cudaStream_t dl_stream = nullptr;
+    cudaEvent_t dl_wait = nullptr;
+    // Device memory of the batch's states and staging buffers: a pool of its own that keeps
+    // freed memory for the next solves instead of returning it to the driver at each
+    // synchronisation, so admitting a solve does not map new memory.
+    cudaMemPool_t pool = nullptr;
     std::string last_error;
     std::vector<SolveRec> solves; // index = id
     std::vector<int> free_ids;
@@ -508,6 +521,29 @@ int mhdb_batch_create(int precision, mhdb_batch** out)
         mhdb::g_create_error = "CUDA: cannot create the batch stream";
         return MHDB_CUDA_ERROR;
     }
+    if (cudaStreamCreateWithFlags(&b->dl_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->dl_wait, cudaEventDisableTiming) != cudaSuccess) {
+        if (b->dl_stream) cudaStreamDestroy(b->dl_stream);
+        cudaStreamDestroy(b->stream);
+        delete b;
+        mhdb::g_create_error = "CUDA: cannot create the batch download stream";
+        return MHDB_CUDA_ERROR;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = b->device;
+    unsigned long long keep = ~0ull;
+    if (cudaMemPoolCreate(&b->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+        if (b->pool) cudaMemPoolDestroy(b->pool);
+        cudaEventDestroy(b->dl_wait);
+        cudaStreamDestroy(b->dl_stream);
+        cudaStreamDestroy(b->stream);
+        delete b;
+        mhdb::g_create_error = "CUDA: cannot create the batch memory pool";
+        return MHDB_CUDA_ERROR;
+    }
     *out = b;
     return MHDB_OK;
 }
@@ -533,7 +569,11 @@ void mhdb_batch_destroy(mhdb_batch* b)
     if (b->ctrl_host) cudaFreeHost(b->ctrl_host);
     if (b->descs) cudaFree(b->descs);
     if (b->work) cudaFree(b->work);
+    cudaStreamSynchronize(b->dl_stream);
+    cudaStreamDestroy(b->dl_stream);
+    cudaEventDestroy(b->dl_wait);
     cudaStreamDestroy(b->stream);
+    cudaMemPoolDestroy(b->pool);
     if (prev >= 0) cudaSetDevice(prev);
     delete b;
 }
@@ -596,21 +636,21 @@ void add_solve(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, 
     s.tiles_x = (grid->nx + tx - 1) / tx;
     s.tiles_y = (grid->ny + ty - 1) / ty;
     const size_t bytes = 9 * s.geom.plane * 8;
-    check(cudaMallocAsync(&s.U, bytes, b->stream), "cudaMallocAsync(U)");
-    const cudaError_t e2 = cudaMallocAsync(&s.Us, bytes, b->stream);
+    check(cudaMallocFromPoolAsync(&s.U, bytes, b->pool, b->stream), "cudaMallocFromPoolAsync(U)");
+    const cudaError_t e2 = cudaMallocFromPoolAsync(&s.Us, bytes, b->pool, b->stream);
     if (e2 != cudaSuccess) {
         cudaFreeAsync(s.U, b->stream);
-        check(e2, "cudaMallocAsync(U*)");
+        check(e2, "cudaMallocFromPoolAsync(U*)");
     }
     s.bytes = 2 * bytes;
     const long long n = static_cast<long long>(grid->nx) * grid->ny;
     if (comps != nullptr) {
         double* stg = nullptr;
-        const cudaError_t e3 = cudaMallocAsync(reinterpret_cast<void**>(&stg), 9 * n_tot * sizeof(double), b->stream);
+        const cudaError_t e3 = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&stg), 9 * n_tot * sizeof(double), b->pool, b->stream);
         if (e3 != cudaSuccess) {
             cudaFreeAsync(s.U, b->stream);
             cudaFreeAsync(s.Us, b->stream);
-            check(e3, "cudaMallocAsync(staging)");
+            check(e3, "cudaMallocFromPoolAsync(staging)");
         }
         for (int c = 0; c < 9; ++c) {
             check(cudaMemcpyAsync(stg + c * n_tot, comps[c], n_tot * sizeof(double),
@@ -759,6 +799,34 @@ int mhdb_batch_step(mhdb_batch* b, int nsteps, int* active)
     });
 }
 
+int mhdb_batch_launch(mhdb_batch* b, int nsteps)
+{
+    return guarded(b, [&] {
+        if (nsteps < 0) {
+            throw BatchFail{MHDB_INVALID_ARGUMENT, "nsteps must be non-negative"};
+        }
+        if (b->precision == MHDB_FP64) {
+            run_steps<PolicyF64>(b, nsteps);
+        } else {
+            run_steps<PolicyMixed>(b, nsteps);
+        }
+    });
+}
+
+int mhdb_batch_poll(mhdb_batch* b, int* active)
+{
+    return guarded(b, [&] {
+        poll(b);
+        if (active != nullptr) {
+            int n = 0;
+            for (const auto& s : b->solves) {
+                n += (s.live && s.last.finished == 0) ? 1 : 0;
+            }
+            *active = n;
+        }
+    });
+}
+
 int mhdb_batch_status(mhdb_batch* b, int id, mhdb_result* result, int* finished)
 {
     return guarded(b, [&] {
@@ -794,25 +862,33 @@ int mhdb_batch_download(mhdb_batch* b, int id, double* const comps[9], size_t n_
         if (comps == nullptr || n_tot != static_cast<size_t>(nxt) * nyt) {
             throw BatchFail{MHDB_INVALID_ARGUMENT, "StateField size does not match Grid2D"};
         }
+        // A solve that the last poll saw finished is final: every write to it completed before
+        // that poll returned, and later steps skip it, so its download does not wait for the
+        // steps in flight. Any other solve waits for everything issued so far.
+        cudaStream_t st = b->dl_stream;
+        if (s.last.finished == 0) {
+            check(cudaEventRecord(b->dl_wait, b->stream), "cudaEventRecord");
+            check(cudaStreamWaitEvent(st, b->dl_wait, 0), "cudaStreamWaitEvent");
+        }
         double* stg = nullptr;
-        check(cudaMallocAsync(reinterpret_cast<void**>(&stg), 9 * n_tot * sizeof(double), b->stream),
-              "cudaMallocAsync(staging)");
+        check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&stg), 9 * n_tot * sizeof(double), b->pool, st),
+              "cudaMallocFromPoolAsync(staging)");
         const long long n = static_cast<long long>(n_tot);
         if (b->precision == MHDB_FP64) {
-            batch_pack<<<blocks_for(n, 256), 256, 0, b->stream>>>(
+            batch_pack<<<blocks_for(n, 256), 256, 0, st>>>(
                 LoadF64{static_cast<const double*>(s.U), s.geom}, stg, s.geom, s.grid.ng, nxt, nyt, n_tot);
         } else {
-            batch_pack<<<blocks_for(n, 256), 256, 0, b->stream>>>(
+            batch_pack<<<blocks_for(n, 256), 256, 0, st>>>(
                 LoadMx{mixed_view(s.U, s.geom), s.geom}, stg, s.geom, s.grid.ng, nxt, nyt, n_tot);
         }
         ++b->launches;
         check(cudaGetLastError(), "batch pack launch");
         for (int c = 0; c < 9; ++c) {
             check(cudaMemcpyAsync(comps[c], stg + c * n_tot, n_tot * sizeof(double),
-                                  cudaMemcpyDeviceToHost, b->stream), "cudaMemcpyAsync(download)");
+                                  cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(download)");
         }
-        check(cudaFreeAsync(stg, b->stream), "cudaFreeAsync(staging)");
-        check(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
+        check(cudaFreeAsync(stg, st), "cudaFreeAsync(staging)");
+        check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     });
 }
 

@@ -45,10 +45,11 @@ struct MarchCfg {
 
 // TMA-fed strip-march configuration (FP32-mixed form only): NW warps per block, LY rows per
 // warp, MINB blocks per SM.
-template <int NW_, int LY_, int MINB_, bool HF_ = true>
+template <int NW_, int LY_, int MINB_, bool HF_ = true, bool ST_ = true>
 struct MarchTmaCfg {
     static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
     static constexpr bool HF = HF_; // wait for the halo row before the x sweep
+    static constexpr bool ST = ST_; // results leave through TMA row stores
     static constexpr bool MARCH_TMA = true;
 };
 
@@ -66,10 +67,10 @@ template <class Policy, class Cfg, int L, bool NI, bool MASK>
 void fill_pair(StageKernels& k)
 {
     if constexpr (is_march_tma<Cfg>::value) {
-        static_assert(!NI && !MASK, "the strip-march kernel serves ideal, unmasked solves");
+        static_assert(!MASK, "the strip-march kernel serves unmasked solves");
         static_assert(sizeof(typename Policy::T) == 4, "the TMA strip march is FP32-mixed only");
-        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF>;
-        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF>;
+        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST, NI>;
+        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST, NI>;
         k.tile_x = Cfg::NW * kMarchOwned;
         k.tile_y = Cfg::LY;
         k.threads = Cfg::NW * 32;
@@ -77,10 +78,10 @@ void fill_pair(StageKernels& k)
         k.smem2 = march_tma_smem_bytes<2>(Cfg::NW);
         return;
     } else if constexpr (is_march<Cfg>::value) {
-        static_assert(!NI && !MASK, "the strip-march kernel serves ideal, unmasked solves");
+        static_assert(!MASK, "the strip-march kernel serves unmasked solves");
         using T = typename Policy::T;
-        auto s1 = march_kernel<Policy, L, 1, Cfg::LY, Cfg::NW, Cfg::MINB>;
-        auto s2 = march_kernel<Policy, L, 2, Cfg::LY, Cfg::NW, Cfg::MINB>;
+        auto s1 = march_kernel<Policy, L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, NI>;
+        auto s2 = march_kernel<Policy, L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, NI>;
         if constexpr (sizeof(T) == 8) {
             k.f64_stage1 = s1;
             k.f64_stage2 = s2;
@@ -123,22 +124,41 @@ StageKernels select_full(int lim, bool ni, bool mask)
     return k;
 }
 
-// Ideal, unmasked kernels only (tuning configurations).
+// Tuning configurations: unmasked solves; the shared-memory tile configurations other than the
+// default serve ideal solves only, the strip-march ones ideal and non-ideal solves.
 template <class Policy, class Cfg>
 StageKernels select_ideal(int lim, bool ni, bool mask)
 {
     StageKernels k;
-    if (ni || mask) {
+    if (mask) {
         return k;
     }
-    if (lim == kMinmod) {
-        fill_pair<Policy, Cfg, kMinmod, false, false>(k);
-    } else if (lim == kMC) {
-        fill_pair<Policy, Cfg, kMC, false, false>(k);
+    if constexpr (is_march<Cfg>::value || is_march_tma<Cfg>::value) {
+#define MHDB_SEL(LL)                                                                               \
+    if (ni) fill_pair<Policy, Cfg, LL, true, false>(k);                                            \
+    else fill_pair<Policy, Cfg, LL, false, false>(k);
+        if (lim == kMinmod) {
+            MHDB_SEL(kMinmod)
+        } else if (lim == kMC) {
+            MHDB_SEL(kMC)
+        } else {
+            MHDB_SEL(kVanLeer)
+        }
+#undef MHDB_SEL
+        return k;
     } else {
-        fill_pair<Policy, Cfg, kVanLeer, false, false>(k);
+        if (ni) {
+            return k;
+        }
+        if (lim == kMinmod) {
+            fill_pair<Policy, Cfg, kMinmod, false, false>(k);
+        } else if (lim == kMC) {
+            fill_pair<Policy, Cfg, kMC, false, false>(k);
+        } else {
+            fill_pair<Policy, Cfg, kVanLeer, false, false>(k);
+        }
+        return k;
     }
-    return k;
 }
 
 } // namespace mhdb

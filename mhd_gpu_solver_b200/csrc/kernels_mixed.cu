@@ -15,17 +15,17 @@ using Cfg7 = MarchCfg<4, 32, 4>;
 using Cfg8 = MarchCfg<4, 128, 4>;
 using Cfg9 = MarchCfg<4, 64, 3>;
 using Cfg10 = MarchTmaCfg<4, 32, 4>;
-using Cfg11 = MarchTmaCfg<4, 32, 5>;
-using Cfg12 = MarchTmaCfg<4, 64, 5>;
-using Cfg13 = MarchTmaCfg<4, 32, 4, false>;
+using Cfg11 = MarchTmaCfg<2, 32, 8>;
+using Cfg12 = MarchTmaCfg<1, 32, 16>;
+using Cfg13 = MarchTmaCfg<4, 32, 4, true, false>;
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
     {32, 16, 256, 2, kKindTileMerged}, {32, 8, 320, 3, kKindTileMerged},
     {112, 64, 128, 4, kKindMarch},     {112, 32, 128, 4, kKindMarch},
     {112, 128, 128, 4, kKindMarch},    {112, 64, 128, 3, kKindMarch},
-    {112, 32, 128, 4, kKindMarchTma},  {112, 32, 128, 5, kKindMarchTma},
-    {112, 64, 128, 5, kKindMarchTma},  {112, 32, 128, 4, kKindMarchTma}};
+    {112, 32, 128, 4, kKindMarchTma},  {56, 32, 64, 8, kKindMarchTma},
+    {28, 32, 32, 16, kKindMarchTma},   {112, 32, 128, 4, kKindMarchTma}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 

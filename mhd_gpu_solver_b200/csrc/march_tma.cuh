@@ -1,4 +1,5 @@
-// TMA-fed warp strip-march stage kernel of the FP32-mixed form (ideal GLM-MHD, no solid mask).
+// TMA-fed warp strip-march stage kernel of the FP32-mixed form (ideal or non-ideal GLM-MHD, no
+// solid mask).
 //
 // The arithmetic is that of march_kernel.cuh (register-resident stencil, shuffle x sweep, every
 // slope limited once and every face evaluated once), so both kernels produce the same values.
@@ -42,7 +43,7 @@ constexpr size_t march_tma_smem_bytes(int warps)
     return static_cast<size_t>(warps) * MarchTmaLayout<STAGE>::kWarpBytes + 128;
 }
 
-template <int L, int STAGE, int LY, bool HF>
+template <int L, int STAGE, int LY, bool HF, bool ST, bool NI>
 __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
                                                   int x0, int y0, int lane, unsigned char* wbase)
 {
@@ -60,6 +61,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     const T inv_gm1 = static_cast<T>(k.inv_gm1);
     const T inv_dx = static_cast<T>(k.inv_dx), inv_dy = static_cast<T>(k.inv_dy);
     const double psi_damp = (c_h64 > 0.0 && k.glm_alpha > 0.0) ? (c_h64 * k.glm_alpha / k.h) : 0.0;
+    const T inv_2dx = static_cast<T>(k.inv_2dx), inv_2dy = static_cast<T>(k.inv_2dy);
 
     const int gx = x0 - 2 + lane;
     const int sx = map_index(gx, g.nx, g.bc_x);
@@ -69,7 +71,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     const int nrows = y1 - y0;
 
     const float* halo_f = reinterpret_cast<const float*>(wbase);
-    const float* own_f = reinterpret_cast<const float*>(wbase + 2 * Lay::kHaloSlot);
+    float* own_f = reinterpret_cast<float*>(wbase + 2 * Lay::kHaloSlot);
     const uint32_t halo_s = smem_addr(wbase);
     const uint32_t own_s = halo_s + 2 * Lay::kHaloSlot;
     const uint32_t bar_s = halo_s + Lay::kBarOff; // halo: +0, +8; own: +16, +24
@@ -120,6 +122,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
 
     // Prologue (direct loads): rows y0-2 .. y0+1, slopes of rows y0-1 and y0, flux G(y0 - 1/2).
     T Wm[9], Wp[9], sYc[9], Gm[9];
+    T Jc[NI ? 3 : 1]; // current of row y (NI)
     {
         Raw r0, r1, r2, r3;
         load(y0 - 2, r0);
@@ -137,6 +140,12 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             sYc[c] = limit_half_slope<L>(Wm[c] - wb[c], Wp[c] - Wm[c]);
         }
         face_flux_regs<T, true, true>(wb, sYm, Wm, sYc, gamma, inv_gm1, c_h, Gm);
+        if constexpr (NI) {
+            T Jb[3];
+            march_current(wa, wb, Wm, inv_2dx, inv_2dy, Jb);
+            march_current(wb, Wm, Wp, inv_2dx, inv_2dy, Jc);
+            march_nonideal_y(Jb, wb, Jc, Wm, k.ni, Gm);
+        }
     }
 
     double smax = 0.0;
@@ -160,6 +169,9 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 sXn[c] = __shfl_down_sync(kFull, sX[c], 1);
             }
             face_flux_regs<T, false, true>(Wm, sX, Wn, sXn, gamma, inv_gm1, c_h, F);
+            if constexpr (NI) {
+                march_nonideal_x(Jc, Wm, Wn, k.ni, F);
+            }
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 dF[c] = F[c] - __shfl_up_sync(kFull, F[c], 1);
@@ -205,8 +217,23 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             sYn[c] = limit_half_slope<L>(Wp[c] - Wm[c], W2[c] - Wp[c]);
         }
         face_flux_regs<T, true, true>(Wm, sYc, Wp, sYn, gamma, inv_gm1, c_h, Gp);
+        T Jn[NI ? 3 : 1];
+        if constexpr (NI) {
+            march_current(Wm, Wp, W2, inv_2dx, inv_2dy, Jn);
+            march_nonideal_y(Jc, Wm, Jn, Wp, k.ni, Gp);
+        }
         // own-cell operands of row y from the own stream, then the stage update
         {
+            if constexpr (ST) {
+                // Row y + 1 goes into the slot of row y - 1 once the store of row y - 1 has read it.
+                if (i >= 1 && i + 1 < nrows) {
+                    if (lane == 0) {
+                        bulk_wait_read_all();
+                        issue_own(i + 1);
+                    }
+                    own_issued = i + 2;
+                }
+            }
             const uint32_t slot = static_cast<uint32_t>(i & 1);
             const bool ok = mbar_wait(bar_s + 16 + 8 * slot, static_cast<uint32_t>((i >> 1) & 1));
             if (__any_sync(kFull, !ok)) {
@@ -214,6 +241,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 break;
             }
             own_done = i + 1;
+            float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
             if (own) {
                 T Lc[9];
 #pragma unroll
@@ -223,14 +251,29 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 if (psi_damp != 0.0) {
                     Lc[8] -= static_cast<float>(psi_damp) * Wm[8]; // include/mhd/rhs.hpp:219-225
                 }
-                const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
-                Policy::template update_ops<STAGE>(a, g, gx, y, false, Lc, dt, k, smax, [&](int q) {
+                auto op = [&](int q) {
                     return q < 18 ? src[q * kTmaOwnW]
                                   : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
-                });
+                };
+                if constexpr (ST) {
+                    // results overwrite this lane's column of the stage-input box (already read)
+                    Policy::template update_ops<STAGE>(a, false, Lc, dt, k, smax, op,
+                                                       [&](int c, float h, float l) {
+                                                           src[c * kTmaOwnW] = h;
+                                                           src[(9 + c) * kTmaOwnW] = l;
+                                                       });
+                    fence_async_smem();
+                } else {
+                    Policy::template update_ops<STAGE>(a, g, gx, y, false, Lc, dt, k, smax, op);
+                }
             }
             __syncwarp();
-            if (i + 2 < nrows) {
+            if constexpr (ST) {
+                if (lane == 0) {
+                    tma_store_3d(&m.out_own, own_s + slot * Lay::kOwnSlot, x0, y, 0);
+                    bulk_commit();
+                }
+            } else if (i + 2 < nrows) {
                 if (lane == 0) {
                     issue_own(i + 2);
                 }
@@ -244,6 +287,18 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             sYc[c] = sYn[c];
             Gm[c] = Gp[c];
         }
+        if constexpr (NI) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                Jc[c] = Jn[c];
+            }
+        }
+    }
+    if constexpr (ST) {
+        if (lane == 0) {
+            bulk_wait_all(); // the row stores have written global memory and read their source
+        }
+        __syncwarp();
     }
     if (failed) {
         // Record the failure and let every copy of this warp land before the CTA can exit.
@@ -261,7 +316,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     return smax;
 }
 
-template <int L, int STAGE, int LY, int NW, int MINB, bool HF>
+template <int L, int STAGE, int LY, int NW, int MINB, bool HF, bool ST, bool NI>
 __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArgsMx a,
                                                                    const __grid_constant__ MarchTmaMaps m)
 {
@@ -276,7 +331,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArg
     const int x0 = (blockIdx.x * NW + warp) * kMarchOwned;
     double smax = 0.0;
     if (x0 < a.geom.nx) { // warp-uniform
-        smax = march_tma_strip<L, STAGE, LY, HF>(a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
+        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
                                              base + warp * MarchTmaLayout<STAGE>::kWarpBytes);
     }
     if constexpr (STAGE == 2) {

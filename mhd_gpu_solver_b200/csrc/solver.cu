@@ -393,8 +393,14 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     s.k = make_consts(h, p);
     const bool ni = s.k.ni_any != 0;
     StageKernels sk{};
-    // Tuned configurations exist for ideal, unmasked solves only; others use configuration 0.
-    const int cfg = (ni || h->has_mask) ? 0 : h->tile_config;
+    // Tuned configurations serve unmasked solves (the tile ones other than 0 ideal solves only,
+    // the strip-march ones non-ideal solves too); every other solve uses configuration 0.
+    int cfg = h->has_mask ? 0 : h->tile_config;
+    if (cfg != 0 && (h->precision == MHDB_FP64 ? select_stage_f64(p->limiter, ni, false, cfg)
+                                               : select_stage_mixed(p->limiter, ni, false, cfg))
+                            .threads == 0) {
+        cfg = 0;
+    }
     if (h->precision == MHDB_FP64) {
         sk = select_stage_f64(p->limiter, ni, h->has_mask, cfg);
         s.s1 = sk.f64_stage1;

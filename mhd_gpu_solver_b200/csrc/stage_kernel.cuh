@@ -148,6 +148,50 @@ __device__ __forceinline__ void face_flux(const T* __restrict__ sS, int sn, int 
     face_flux_regs<T, YDIR>(lc, sl, rc, sr, gamma, inv_gm1, c_h, out);
 }
 
+// Non-ideal correction of one face flux from the cell-centred current J and field B of its two
+// cells (l: left/below, r: right/above): face averages, E from Ohm's law, then the x-face
+// (F_by -= Ez, F_bz += Ey, F_E += By Ez - Bz Ey) or y-face (G_bx += Ez, G_bz -= Ex,
+// G_E += Bz Ex - Bx Ez) update; include/mhd/rhs.hpp:75-114.
+template <class T, bool YDIR>
+__device__ __forceinline__ void add_nonideal_face(T jxl, T jyl, T jzl, T jxr, T jyr, T jzr, T bxl,
+                                                  T byl, T bzl, T bxr, T byr, T bzr,
+                                                  const NonIdealCoef& ni, T (&out)[9])
+{
+    const T Jx = T(0.5) * (jxl + jxr);
+    const T Jy = T(0.5) * (jyl + jyr);
+    const T Jz = T(0.5) * (jzl + jzr);
+    const T Bx = T(0.5) * (bxl + bxr);
+    const T By = T(0.5) * (byl + byr);
+    const T Bz = T(0.5) * (bzl + bzr);
+    T Ex, Ey, Ez;
+    nonideal_e(Jx, Jy, Jz, Bx, By, Bz, ni, Ex, Ey, Ez);
+    if (!YDIR) {
+        out[6] += -Ez;
+        out[7] += Ey;
+        out[4] += By * Ez - Bz * Ey;
+    } else {
+        out[5] += Ez;
+        out[7] += -Ex;
+        out[4] += Bz * Ex - Bx * Ez;
+    }
+}
+
+// Cell-centred current J = curl B of one cell from its four neighbours' field components
+// (include/mhd/nonideal.hpp:30-60): Jx = dBz/dy, Jy = -dBz/dx, Jz = dBy/dx - dBx/dy, central
+// differences.
+template <class T>
+__device__ __forceinline__ void cell_current(T bz_n, T bz_s, T bz_e, T bz_w, T by_e, T by_w,
+                                             T bx_n, T bx_s, T inv_2dx, T inv_2dy, T (&J)[3])
+{
+    const T dbz_dy = (bz_n - bz_s) * inv_2dy;
+    const T dbz_dx = (bz_e - bz_w) * inv_2dx;
+    const T dby_dx = (by_e - by_w) * inv_2dx;
+    const T dbx_dy = (bx_n - bx_s) * inv_2dy;
+    J[0] = dbz_dy;
+    J[1] = -dbz_dx;
+    J[2] = dby_dx - dbx_dy;
+}
+
 // One face of a sweep: flux (HLL + GLM + non-ideal E) into sF[c * fn + t]; sS/sn are the
 // slopes of the same sweep (x: region width TX+2; y: width TX).
 template <class T, int TX, int TY, bool YDIR, bool NI>
@@ -170,26 +214,12 @@ __device__ __forceinline__ void face_item(const T* __restrict__ sW, const T* __r
     T out[9];
     face_flux<T, YDIR>(sS, sn, il, ir, sW, S::NH, wl, wr, gamma, inv_gm1, c_h, out);
     if constexpr (NI) {
-        // Face-averaged J and B, E from Ohm's law (include/mhd/rhs.hpp:75-114).
         const int jr = (fy + 1) * S::JX + (fx + 1);
         const int jl = jr - (YDIR ? S::JX : 1);
-        const T Jx = T(0.5) * (sJ[jl] + sJ[jr]);
-        const T Jy = T(0.5) * (sJ[S::NJ + jl] + sJ[S::NJ + jr]);
-        const T Jz = T(0.5) * (sJ[2 * S::NJ + jl] + sJ[2 * S::NJ + jr]);
-        const T Bx = T(0.5) * (sW[5 * S::NH + wl] + sW[5 * S::NH + wr]);
-        const T By = T(0.5) * (sW[6 * S::NH + wl] + sW[6 * S::NH + wr]);
-        const T Bz = T(0.5) * (sW[7 * S::NH + wl] + sW[7 * S::NH + wr]);
-        T Ex, Ey, Ez;
-        nonideal_e(Jx, Jy, Jz, Bx, By, Bz, ni, Ex, Ey, Ez);
-        if (!YDIR) {
-            out[6] += -Ez;
-            out[7] += Ey;
-            out[4] += By * Ez - Bz * Ey;
-        } else {
-            out[5] += Ez;
-            out[7] += -Ex;
-            out[4] += Bz * Ex - Bx * Ez;
-        }
+        add_nonideal_face<T, YDIR>(sJ[jl], sJ[S::NJ + jl], sJ[2 * S::NJ + jl], sJ[jr],
+                                   sJ[S::NJ + jr], sJ[2 * S::NJ + jr], sW[5 * S::NH + wl],
+                                   sW[6 * S::NH + wl], sW[7 * S::NH + wl], sW[5 * S::NH + wr],
+                                   sW[6 * S::NH + wr], sW[7 * S::NH + wr], ni, out);
     }
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
@@ -304,13 +334,12 @@ __device__ __forceinline__ double stage_tile(const typename Policy::Args& a, int
         const T* bx = sW + 5 * S::NH;
         const T* by = sW + 6 * S::NH;
         const T* bz = sW + 7 * S::NH;
-        const T dbz_dy = (bz[i + HX] - bz[i - HX]) * inv_2dy;
-        const T dbz_dx = (bz[i + 1] - bz[i - 1]) * inv_2dx;
-        const T dby_dx = (by[i + 1] - by[i - 1]) * inv_2dx;
-        const T dbx_dy = (bx[i + HX] - bx[i - HX]) * inv_2dy;
-        sJ[0 * S::NJ + t] = dbz_dy;
-        sJ[1 * S::NJ + t] = -dbz_dx;
-        sJ[2 * S::NJ + t] = dby_dx - dbx_dy;
+        T J[3];
+        cell_current(bz[i + HX], bz[i - HX], bz[i + 1], bz[i - 1], by[i + 1], by[i - 1],
+                     bx[i + HX], bx[i - HX], inv_2dx, inv_2dy, J);
+        sJ[0 * S::NJ + t] = J[0];
+        sJ[1 * S::NJ + t] = J[1];
+        sJ[2 * S::NJ + t] = J[2];
     };
 
     T dFx[R][9];

@@ -187,7 +187,6 @@ struct PolicyMixed {
                 L[c] = 0.0f;
             }
         }
-        const float dtf = static_cast<float>(dt);
         const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
         if (MASK && solid && a.walls) {
             // Rare path in FP64: stage 1 stores fill(U^n); stage 2 stores
@@ -228,11 +227,23 @@ struct PolicyMixed {
                                                       double dt, const Consts& k, double& smax,
                                                       const Op& op)
     {
-        const float dtf = static_cast<float>(dt);
         const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
         float* __restrict__ oh = a.out.hi + o;
         float* __restrict__ ol = a.out.lo + o;
         const size_t pl = g.plane;
+        update_ops<STAGE>(a, solid, L, dt, k, smax, op, [&](int c, float h, float l) {
+            oh[c * pl] = h;
+            ol[c * pl] = l;
+        });
+    }
+    // The same with the results handed to st(c, hi, lo) instead of stored to the output planes.
+    template <int STAGE, class Op, class St>
+    static __device__ __forceinline__ void update_ops(const Args& a, bool solid,
+                                                      const float (&L)[9], double dt,
+                                                      const Consts& k, double& smax, const Op& op,
+                                                      const St& st)
+    {
+        const float dtf = static_cast<float>(dt);
         float xh[9], xl[9];
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
@@ -246,8 +257,7 @@ struct PolicyMixed {
                 float s, e, h, l;
                 two_sum(xh[c], __fmul_rn(dtf, L[c]), s, e); // product rounded first: exact two-sum
                 fast_two_sum(s, xl[c] + e, h, l);
-                oh[c * pl] = h;
-                ol[c * pl] = l;
+                st(c, h, l);
             }
         } else {
             // U^{n+1} = (U^n + U*)/2 + (dt/2) L = U^n + d with d = (U* - U^n)/2 + (dt/2) L,
@@ -270,8 +280,7 @@ struct PolicyMixed {
                                                                     __fsub_rn(xl[c], nl[c]))));
                 two_sum(nh[c], d, s, e);
                 fast_two_sum(s, nl[c] + e, h, l);
-                oh[c * pl] = h;
-                ol[c * pl] = l;
+                st(c, h, l);
                 rf[c] = h;
             }
             if (!solid) {

@@ -1,9 +1,11 @@
-// Tensor-memory-accelerator (TMA) bulk copies into shared memory, completed on mbarriers.
+// Tensor-memory-accelerator (TMA) bulk copies between global and shared memory.
 //
-// Only tiled, non-multicast loads of this GPU's own memory are issued (cp.async.bulk.tensor
-// .3d.shared::cluster.global.mbarrier::complete_tx::bytes; a CTA launched without a cluster is a
-// cluster of one). Every wait is bounded: mbar_wait gives up after kWaitNs of global-timer time
-// and returns false, so a kernel can record the failure and drain its copies instead of spinning.
+// Loads are tiled, non-multicast loads of this GPU's own memory
+// (cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes; a CTA launched
+// without a cluster is a cluster of one), completed on mbarriers. Stores are tiled bulk stores
+// tracked by bulk groups. Every mbarrier wait is bounded: mbar_wait gives up after kWaitNs of
+// global-timer time and returns false, so a kernel can record the failure and drain its copies
+// instead of spinning.
 #pragma once
 
 #include <cuda.h>
@@ -98,6 +100,39 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
                  " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
                  "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
                  : "memory");
+}
+
+// 3D tiled store of one box from shared memory at src to (x, y, z) of the tensor map; elements
+// outside the tensor's extent are not written. Completion is tracked by bulk groups.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int x, int y,
+                                             int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// All committed bulk stores of this thread have finished reading their shared-memory source.
+__device__ __forceinline__ void bulk_wait_read_all()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// All committed bulk stores of this thread are complete (their global writes performed).
+__device__ __forceinline__ void bulk_wait_all()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory writes before later async-proxy (TMA) reads.
+__device__ __forceinline__ void fence_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 } // namespace mhdb

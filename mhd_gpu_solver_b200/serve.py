@@ -9,8 +9,8 @@ The loop
 * advances every admitted, unfinished request together: each chunk of RK2 steps is one
   persistent launch per stage over all of them, so requests that arrive while others are on the
   GPU join the next chunk (continuous batching);
-* when a request finishes, downloads its result, frees its memory and records its latency
-  (completion minus arrival).
+* when a request finishes, downloads its result while the next chunk runs, frees its memory and
+  records its latency (completion minus arrival).
 
 ``serve_one_at_a_time`` runs the same requests through the plain FP64 single-solve path, one after
 the other, as the comparison. ``make_stream`` draws a seeded request stream: Poisson arrivals,
@@ -93,6 +93,33 @@ def make_stream(n_requests: int, rate: float, seed: int = 0, side=(128, 2048),
     return out
 
 
+class ResultBuffer:
+    """One page-locked host buffer, grown to the largest result seen, that results are copied
+    into before they are handed on (a fresh array per result would fault its pages in during
+    every copy). Both serving paths use it, so they pay the same host-side cost."""
+
+    def __init__(self):
+        self._flat = np.empty(0, dtype=np.float64)
+        self._pinned = None
+
+    def view(self, shape) -> np.ndarray:
+        n = int(np.prod(shape))
+        if n > self._flat.size:
+            try:
+                import torch
+
+                self._pinned = torch.empty(n, dtype=torch.float64, pin_memory=True)
+                self._flat = self._pinned.numpy()
+            except (ImportError, RuntimeError):
+                self._pinned = None
+                self._flat = np.empty(n, dtype=np.float64)
+        return self._flat[:n].reshape(shape)
+
+
+def _result_shape(n: int, ng: int = 2):
+    return (9, n + 2 * ng, n + 2 * ng)
+
+
 @dataclass
 class ServeStats:
     completions: list = field(default_factory=list)
@@ -119,13 +146,15 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
     """Serve a request stream in real time with continuous batching."""
     batch = BatchSolver(precision)
     stats = ServeStats()
+    results = ResultBuffer()
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     queue: deque[Request] = deque()
-    active: dict[int, tuple[Request, float]] = {}
+    active: dict[int, tuple[Request, float]] = {}  # admitted, not finished at the last poll
+    done: list = []  # (sid, request, admitted, result, poll time) finished at the last poll
     in_use = 0
     start = time.perf_counter()
     try:
-        while pending or queue or active:
+        while pending or queue or active or done:
             now = time.perf_counter() - start
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
@@ -133,7 +162,7 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
             while queue:
                 req = queue[0]
                 need = state_bytes(req.n, req.n)
-                if in_use + need > memory_cap and active:
+                if in_use + need > memory_cap and (active or done):
                     break
                 queue.popleft()
                 sid = batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
@@ -141,28 +170,32 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
                 active[sid] = (req, time.perf_counter() - start)
             stats.peak_bytes = max(stats.peak_bytes, in_use)
             stats.max_active = max(stats.max_active, len(active))
-            if not active:
+            if not active and not done:
                 if pending:
                     time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - start)))
                 continue
-            batch.step(chunk)
-            stats.chunks += 1
-            done_at = time.perf_counter() - start
-            for sid in list(active):
-                r, fin = batch.status(sid)
-                if not fin:
-                    continue
-                req, admitted = active.pop(sid)
+            if active:
+                batch.launch(chunk)  # the next chunk runs while finished requests leave
+                stats.chunks += 1
+            for sid, req, admitted, r, polled in done:
                 if download or keep_states:
-                    out = batch.download(sid)
+                    out = batch.download(sid, out=results.view(_result_shape(req.n)))
                     if keep_states:
-                        stats.states[req.rid] = out
+                        stats.states[req.rid] = out.copy()
                 stats.completions.append(Completion(req.rid, req.arrival, admitted,
                                                     time.perf_counter() - start if download
-                                                    else done_at, r.steps, r.t,
-                                                    req.n * req.n))
+                                                    else polled, r.steps, r.t, req.n * req.n))
                 batch.remove(sid)
                 in_use -= state_bytes(req.n, req.n)
+            done = []
+            if active:
+                batch.poll()
+                polled = time.perf_counter() - start
+                for sid in list(active):
+                    r, fin = batch.status(sid)
+                    if fin:
+                        req, admitted = active.pop(sid)
+                        done.append((sid, req, admitted, r, polled))
         stats.makespan = time.perf_counter() - start
     finally:
         batch.close()
@@ -174,6 +207,7 @@ def serve_one_at_a_time(requests: list[Request], precision: int = _capi.FP64,
     """The same stream through the plain single-solve path, one request at a time, in arrival
     order (a request waits until it has arrived and the previous one has finished)."""
     stats = ServeStats()
+    results = ResultBuffer()
     start = time.perf_counter()
     for req in sorted(requests, key=lambda r: r.arrival):
         now = time.perf_counter() - start
@@ -187,9 +221,9 @@ def serve_one_at_a_time(requests: list[Request], precision: int = _capi.FP64,
             dev.generate(req.init(), params)
             r = dev.solve(params)
             if download or keep_states:
-                out = dev.download()
+                out = dev.download(out=results.view(_result_shape(req.n)))
                 if keep_states:
-                    stats.states[req.rid] = out
+                    stats.states[req.rid] = out.copy()
         finally:
             dev.close()
         stats.completions.append(Completion(req.rid, req.arrival, admitted,

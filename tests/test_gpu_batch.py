@@ -175,3 +175,38 @@ def test_device_generator_matches_host_generator(kind, precision):
     sid = b.add_generated(nx, ny, spec, fixed_params(0, gamma=gamma), (0, 0), fixed_steps=True)
     assert np.array_equal(b.download(sid), got)
     b.close()
+
+
+def test_launch_poll_and_downloads_beside_running_steps():
+    """mhdb_batch_launch / mhdb_batch_poll give the results of mhdb_batch_step, and a solve that
+    a poll reported finished downloads unchanged while the next steps of the others run."""
+    steps = [12, 30, 45]
+    cases = [CASES[0], CASES[1], CASES[4]]
+    states = [state(c[0], c[1], 40 + i, c[2], c[3], c[6]) for i, c in enumerate(cases)]
+
+    ref_b = BatchSolver(_capi.FP32)
+    ref_ids = [ref_b.add(U, fixed_params(n, **params_of(c)), c[3], fixed_steps=True)
+               for U, n, c in zip(states, steps, cases)]
+    while ref_b.step(8) > 0:
+        pass
+    refs = [ref_b.download(i) for i in ref_ids]
+    ref_b.close()
+
+    b = BatchSolver(_capi.FP32)
+    ids = [b.add(U, fixed_params(n, **params_of(c)), c[3], fixed_steps=True)
+           for U, n, c in zip(states, steps, cases)]
+    got, done = {}, []
+    active = len(ids)
+    while active > 0 or done:
+        if active > 0:
+            b.launch(8)
+        for sid in done:  # finished at the previous poll; the next chunk is in flight
+            got[sid] = b.download(sid)
+            b.remove(sid)
+        done = []
+        if active > 0:
+            active = b.poll()
+            done = [sid for sid in ids if sid not in got and b.status(sid)[1]]
+    b.close()
+    for sid, ref in zip(ids, refs):
+        assert np.array_equal(got[sid], ref)

@@ -363,3 +363,34 @@ def test_tma_strip_march_equals_register_strip_march(case):
         r, got = run(cfg)
         assert r.steps == r0.steps and r.t == r0.t, cfg
         assert np.array_equal(got, ref), (cfg, float(np.max(np.abs(got - ref))))
+
+
+NI_PARAMS = dict(ohmic=True, hall=True, ambipolar=True, eta_ohm=1e-3, eta_hall=1e-2,
+                 eta_ambipolar=1e-3)
+
+
+@pytest.mark.parametrize("precision", [_capi.FP64, _capi.FP32])
+@pytest.mark.parametrize("case", [0, 1, 2, 4])
+def test_nonideal_strip_march_configurations_match_oracle(precision, case):
+    """Ohmic, Hall and ambipolar terms in the strip-march kernels (current carried row to row,
+    x neighbours by shuffle): FP64 to 1e-12, FP32-mixed to 1e-6 against the FP64 oracle."""
+    nx, ny, bcx, bcy, state, lim = MARCH_CASES[case]
+    bc = (bcx, bcy)
+    prim = (wl.fourier_state(nx, ny, 9) if state == "fourier" else wl.four_quadrant(nx, ny, 3))
+    U0 = initial_state(prim, 5.0 / 3.0, bc)
+    p = orc.Params(limiter=lim, max_steps=20, fixed_steps=True, **NI_PARAMS)
+    ref, tr, sr, _ = orc.solve(U0, orc.Grid(nx, ny), p, bc)
+    tol = FP64_L1 if precision == _capi.FP64 else MIXED_L1
+    marches = [c for c in _capi.tile_configs(precision) if c["kind"].startswith("march")]
+    for cfg in marches:
+        dev = _capi.DeviceSolver(nx, ny, precision=precision)
+        dev.set_tile_config(cfg["config"])
+        dev.configure(bcx, bcy)
+        dev.upload(U0)
+        r = dev.solve_steps(_capi.make_params(limiter=lim, **NI_PARAMS), 20)
+        got = dev.download()
+        dev.close()
+        assert r.steps == sr
+        assert abs(r.t - tr) <= (1e-12 if precision == _capi.FP64 else 1e-6) * max(1.0, tr)
+        err = rel_l1(got, ref)
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (cfg, err)
