@@ -45,11 +45,12 @@ struct MarchCfg {
 
 // TMA-fed strip-march configuration (FP32-mixed form only): NW warps per block, LY rows per
 // warp, MINB blocks per SM.
-template <int NW_, int LY_, int MINB_, bool HF_ = true, bool ST_ = true>
+template <int NW_, int LY_, int MINB_, bool HF_ = true, bool ST1_ = true, bool ST2_ = false>
 struct MarchTmaCfg {
     static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
-    static constexpr bool HF = HF_; // wait for the halo row before the x sweep
-    static constexpr bool ST = ST_; // results leave through TMA row stores
+    static constexpr bool HF = HF_;   // wait for the halo row before the x sweep
+    static constexpr bool ST1 = ST1_; // stage 1 results leave through TMA row stores
+    static constexpr bool ST2 = ST2_; // the same for stage 2
     static constexpr bool MARCH_TMA = true;
 };
 
@@ -69,13 +70,13 @@ void fill_pair(StageKernels& k)
     if constexpr (is_march_tma<Cfg>::value) {
         static_assert(!MASK, "the strip-march kernel serves unmasked solves");
         static_assert(sizeof(typename Policy::T) == 4, "the TMA strip march is FP32-mixed only");
-        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST, NI>;
-        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST, NI>;
+        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI>;
+        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI>;
         k.tile_x = Cfg::NW * kMarchOwned;
         k.tile_y = Cfg::LY;
         k.threads = Cfg::NW * 32;
-        k.smem = march_tma_smem_bytes<1>(Cfg::NW);
-        k.smem2 = march_tma_smem_bytes<2>(Cfg::NW);
+        k.smem = march_tma_smem_bytes<1, Cfg::ST1>(Cfg::NW);
+        k.smem2 = march_tma_smem_bytes<2, Cfg::ST2>(Cfg::NW);
         return;
     } else if constexpr (is_march<Cfg>::value) {
         static_assert(!MASK, "the strip-march kernel serves unmasked solves");

@@ -10,22 +10,21 @@ using Cfg2 = TileCfg<32, 8, 256, 3>;
 using Cfg3 = TileCfg<32, 16, 384, 2, true>;
 using Cfg4 = TileCfg<32, 16, 256, 2, true>;
 using Cfg5 = TileCfg<32, 8, 320, 3, true>;
-using Cfg6 = MarchCfg<4, 64, 4>;
-using Cfg7 = MarchCfg<4, 32, 4>;
-using Cfg8 = MarchCfg<4, 128, 4>;
-using Cfg9 = MarchCfg<4, 64, 3>;
-using Cfg10 = MarchTmaCfg<4, 32, 4>;
-using Cfg11 = MarchTmaCfg<2, 32, 8>;
-using Cfg12 = MarchTmaCfg<1, 32, 16>;
-using Cfg13 = MarchTmaCfg<4, 32, 4, true, false>;
+using Cfg6 = MarchCfg<4, 64, 3>;
+using Cfg7 = MarchTmaCfg<4, 32, 4>;
+using Cfg8 = MarchTmaCfg<2, 32, 8>;
+using Cfg9 = MarchTmaCfg<1, 32, 16>;
+using Cfg10 = MarchTmaCfg<4, 32, 4, true, false>;
+using Cfg11 = MarchTmaCfg<1, 32, 16, true, false>;
+using Cfg12 = MarchTmaCfg<1, 64, 16>;
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
     {32, 16, 256, 2, kKindTileMerged}, {32, 8, 320, 3, kKindTileMerged},
-    {112, 64, 128, 4, kKindMarch},     {112, 32, 128, 4, kKindMarch},
-    {112, 128, 128, 4, kKindMarch},    {112, 64, 128, 3, kKindMarch},
-    {112, 32, 128, 4, kKindMarchTma},  {56, 32, 64, 8, kKindMarchTma},
-    {28, 32, 32, 16, kKindMarchTma},   {112, 32, 128, 4, kKindMarchTma}};
+    {112, 64, 128, 3, kKindMarch},     {112, 32, 128, 4, kKindMarchTma},
+    {56, 32, 64, 8, kKindMarchTma},    {28, 32, 32, 16, kKindMarchTma},
+    {112, 32, 128, 4, kKindMarchTma},  {28, 32, 32, 16, kKindMarchTma},
+    {28, 64, 32, 16, kKindMarchTma}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -60,8 +59,6 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_ideal<PolicyMixed, Cfg11>(limiter, nonideal, mask);
     case 12:
         return select_ideal<PolicyMixed, Cfg12>(limiter, nonideal, mask);
-    case 13:
-        return select_ideal<PolicyMixed, Cfg13>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

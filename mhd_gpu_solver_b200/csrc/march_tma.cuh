@@ -23,7 +23,9 @@
 
 namespace mhdb {
 
-template <int STAGE>
+// Shared memory of one warp: 2 halo slots, 2 own slots, (ST) one staging slot for the row store,
+// then the 4 mbarriers.
+template <int STAGE, bool ST>
 struct MarchTmaLayout {
     static constexpr int kHaloFloats = 9 * kTmaHaloW;             // 324 floats, 1296 B
     static constexpr int kHaloBytes = kHaloFloats * 4;
@@ -33,14 +35,15 @@ struct MarchTmaLayout {
     static constexpr int kOwnBoxes = STAGE == 1 ? 1 : 2;
     static constexpr int kOwnSlot = kOwnBoxes * kOwnBoxSlot;
     static constexpr int kOwnTx = kOwnBoxes * kOwnBoxBytes;       // transaction bytes per row
-    static constexpr int kBarOff = 2 * kHaloSlot + 2 * kOwnSlot;
+    static constexpr int kStageOff = 2 * kHaloSlot + 2 * kOwnSlot;
+    static constexpr int kBarOff = kStageOff + (ST ? kOwnBoxSlot : 0);
     static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
 };
 
-template <int STAGE>
+template <int STAGE, bool ST>
 constexpr size_t march_tma_smem_bytes(int warps)
 {
-    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE>::kWarpBytes + 128;
+    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST>::kWarpBytes + 128;
 }
 
 template <int L, int STAGE, int LY, bool HF, bool ST, bool NI>
@@ -50,7 +53,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     using Policy = PolicyMixed;
     using T = float;
     using Raw = Policy::Raw;
-    using Lay = MarchTmaLayout<STAGE>;
+    using Lay = MarchTmaLayout<STAGE, ST>;
     constexpr unsigned kFull = 0xffffffffu;
     const Geometry& g = a.geom;
     const Consts& k = a.k;
@@ -71,9 +74,11 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     const int nrows = y1 - y0;
 
     const float* halo_f = reinterpret_cast<const float*>(wbase);
-    float* own_f = reinterpret_cast<float*>(wbase + 2 * Lay::kHaloSlot);
+    const float* own_f = reinterpret_cast<const float*>(wbase + 2 * Lay::kHaloSlot);
+    float* stg_f = reinterpret_cast<float*>(wbase + Lay::kStageOff);
     const uint32_t halo_s = smem_addr(wbase);
     const uint32_t own_s = halo_s + 2 * Lay::kHaloSlot;
+    const uint32_t stg_s = halo_s + Lay::kStageOff;
     const uint32_t bar_s = halo_s + Lay::kBarOff; // halo: +0, +8; own: +16, +24
 
     if (lane == 0) {
@@ -224,16 +229,6 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
         }
         // own-cell operands of row y from the own stream, then the stage update
         {
-            if constexpr (ST) {
-                // Row y + 1 goes into the slot of row y - 1 once the store of row y - 1 has read it.
-                if (i >= 1 && i + 1 < nrows) {
-                    if (lane == 0) {
-                        bulk_wait_read_all();
-                        issue_own(i + 1);
-                    }
-                    own_issued = i + 2;
-                }
-            }
             const uint32_t slot = static_cast<uint32_t>(i & 1);
             const bool ok = mbar_wait(bar_s + 16 + 8 * slot, static_cast<uint32_t>((i >> 1) & 1));
             if (__any_sync(kFull, !ok)) {
@@ -241,7 +236,13 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 break;
             }
             own_done = i + 1;
-            float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
+            if constexpr (ST) {
+                if (lane == 0) {
+                    bulk_wait_read_all(); // the store of row y - 1 has read the staging slot
+                }
+                __syncwarp();
+            }
+            const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
             if (own) {
                 T Lc[9];
 #pragma unroll
@@ -256,11 +257,11 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                                   : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
                 };
                 if constexpr (ST) {
-                    // results overwrite this lane's column of the stage-input box (already read)
+                    float* dst = stg_f + (lane - 2);
                     Policy::template update_ops<STAGE>(a, false, Lc, dt, k, smax, op,
                                                        [&](int c, float h, float l) {
-                                                           src[c * kTmaOwnW] = h;
-                                                           src[(9 + c) * kTmaOwnW] = l;
+                                                           dst[c * kTmaOwnW] = h;
+                                                           dst[(9 + c) * kTmaOwnW] = l;
                                                        });
                     fence_async_smem();
                 } else {
@@ -268,15 +269,16 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 }
             }
             __syncwarp();
-            if constexpr (ST) {
-                if (lane == 0) {
-                    tma_store_3d(&m.out_own, own_s + slot * Lay::kOwnSlot, x0, y, 0);
+            if (lane == 0) {
+                if constexpr (ST) {
+                    tma_store_3d(&m.out_own, stg_s, x0, y, 0);
                     bulk_commit();
                 }
-            } else if (i + 2 < nrows) {
-                if (lane == 0) {
+                if (i + 2 < nrows) {
                     issue_own(i + 2);
                 }
+            }
+            if (i + 2 < nrows) {
                 own_issued = i + 3;
             }
         }
@@ -332,7 +334,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArg
     double smax = 0.0;
     if (x0 < a.geom.nx) { // warp-uniform
         smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
-                                             base + warp * MarchTmaLayout<STAGE>::kWarpBytes);
+                                             base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes);
     }
     if constexpr (STAGE == 2) {
         reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
