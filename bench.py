@@ -12,7 +12,8 @@ zone-updates/s (interior cells x steps / device seconds).
 * ``roofline``: the dominant stage kernel's algorithmic bytes per launch (9 fields x 8 B:
   stage 1 reads U and writes U*, 144 B/cell; stage 2 reads U* and U and writes U, 216 B/cell;
   360 B per zone-update) over its average event-timed duration, against the measured HBM copy
-  bandwidth.
+  bandwidth; ``traffic`` = that kernel's DRAM bytes per launch from the committed ncu capture of
+  the same kernel kind (profiles/stage_traffic.json, bytes per cell x cells).
 * ``cpu_baseline``: the reference CPU solver (SIMD + threads), compiled from the reference's
   own headers into oracle/_ref, on all host cores, on a bounded number of steps of the same
   4096^2 state (MC limiter: the reference has no van Leer).
@@ -158,6 +159,21 @@ def measured_hbm_peak() -> tuple[float, str]:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def measured_traffic(kind: str, stage: int, cells: float):
+    """DRAM bytes (read + write) of one stage launch, scaled by cells from the per-cell figure of
+    the committed ncu capture of that kernel kind (traffic grows in proportion to the cells), or
+    None when no capture of this kind is committed."""
+    path = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    try:
+        with open(path) as f:
+            prof = json.load(f)
+    except (OSError, ValueError):
+        return None, None
+    if prof.get("kind") != kind:
+        return None, None
+    return prof["dram_bytes_per_cell"][f"stage{stage}"] * cells, prof.get("source")
 
 
 def time_form(dev, params, steps: int, warmup: int, n: int) -> dict:
@@ -435,6 +451,8 @@ def main():
     peak, peak_kind = measured_hbm_peak()
     dom = 2 if mixed["prof"]["stage2_ms"] >= mixed["prof"]["stage1_ms"] else 1
     achieved = mixed[f"stage{dom}_gbs"]
+    mixed_cfg = next(c for c in _capi.tile_configs(_capi.FP32) if c["config"] == chosen["fp32_mixed"])
+    traffic, traffic_src = measured_traffic(mixed_cfg["kind"], dom, float(n) * n)
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -454,7 +472,8 @@ def main():
         "speedup_fp32_mixed_over_fp64": results["fp64"]["ms_max"] / ms,
         "roofline": {"bound": "hbm", "kernel": f"stage{dom} (fp32_mixed)", "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None, "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "algorithmic_bytes_per_launch": BYTES_STAGE[dom] * n * n,
                      "stage1_avg_ms": mixed["stage1_avg_ms"],
                      "stage2_avg_ms": mixed["stage2_avg_ms"]},
