@@ -207,6 +207,18 @@ int mhdb_batch_step(mhdb_batch* b, int nsteps, int* active);
 int mhdb_batch_launch(mhdb_batch* b, int nsteps);
 int mhdb_batch_poll(mhdb_batch* b, int* active);
 
+/* Batch configurations: the kernel a solve runs with in a batch (tile shape, halo staging and
+   threads per work item). mhdb_batch_config_info writes the interior cells of one work item
+   (tile width and height), its threads and its kernel kind (MHDB_KERNEL_*). FP32-mixed: 0 = TMA
+   strip march, one warp by 32 rows; 1 = register strip march, 4 warps by 32 rows; 2 = TMA strip
+   march, one warp by 64 rows. mhdb_batch_set_config picks one for a solve (-1: by the solve's
+   size, the default); the batch autotuner (mhd_gpu_solver_b200.autotune.tune_batch) chooses per
+   size class. The configurations agree to the FP32 rounding of the form. */
+int mhdb_batch_config_count(int precision);
+int mhdb_batch_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
+                           int* kind);
+int mhdb_batch_set_config(mhdb_batch* b, int id, int config);
+
 /* t, steps, c_h and whether the solve has finished; MHDB_MAX_STEPS / MHDB_BAD_TIMESTEP as
    mhdb_solve would report them. */
 int mhdb_batch_status(mhdb_batch* b, int id, mhdb_result* result, int* finished);

@@ -30,7 +30,8 @@ EXPORTS = (
     "mhdb_batch_create", "mhdb_batch_destroy", "mhdb_batch_last_error", "mhdb_batch_add",
     "mhdb_batch_remove", "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download",
     "mhdb_batch_info", "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
-    "mhdb_batch_launch", "mhdb_batch_poll",
+    "mhdb_batch_launch", "mhdb_batch_poll", "mhdb_batch_config_count", "mhdb_batch_config_info",
+    "mhdb_batch_set_config",
 )
 
 
@@ -45,6 +46,13 @@ class Params(C.Structure):
                 ("hall", C.c_int), ("ambipolar", C.c_int), ("eta_ohm", C.c_double),
                 ("eta_hall", C.c_double), ("eta_ambipolar", C.c_double),
                 ("max_steps", C.c_int)]
+
+
+def nonideal_any(p: Params) -> bool:
+    """Whether the non-ideal terms are on: a flag set and its coefficient non-zero
+    (include/physics_config/mhd_config.hpp:90-94)."""
+    return bool((p.ohmic and p.eta_ohm != 0.0) or (p.hall and p.eta_hall != 0.0)
+                or (p.ambipolar and p.eta_ambipolar != 0.0))
 
 
 class Result(C.Structure):
@@ -113,6 +121,10 @@ def _load() -> C.CDLL:
         "mhdb_batch_remove": ([b, C.c_int], C.c_int),
         "mhdb_batch_step": ([b, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_launch": ([b, C.c_int], C.c_int),
+        "mhdb_batch_config_count": ([C.c_int], C.c_int),
+        "mhdb_batch_config_info": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "mhdb_batch_set_config": ([b, C.c_int, C.c_int], C.c_int),
         "mhdb_batch_poll": ([b, C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_status": ([b, C.c_int, C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_download": ([b, C.c_int, _PPD, C.c_size_t], C.c_int),

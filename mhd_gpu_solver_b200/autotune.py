@@ -8,6 +8,11 @@ remembers the fastest. Results are cached in memory for the process and can be s
 from a JSON file. Configurations other than 0 serve unmasked solves (the strip-march ones ideal
 and non-ideal solves, the other tile ones ideal solves only); a solve that the chosen
 configuration does not serve runs configuration 0.
+
+``tune_batch`` does the same for the batched form: per (precision, limiter, ideal or non-ideal,
+size class) it times every batch configuration (``batch.batch_configs``: strip march with or
+without TMA staging of the rows, work-item shapes) on a batch of same-class solves that fills the
+GPU, and remembers the fastest; ``BatchSolver(tune=True)`` applies the choice to each solve.
 """
 
 from __future__ import annotations
@@ -71,6 +76,55 @@ def tune(precision: int, limiter: int, nx: int, ny: int, steps: int = 6,
 
         apply_boundary_conditions(state, n, n, 2, 0, 0)
         times = {c["config"]: _time_config(precision, limiter, n, n, c["config"], state, steps)
+                 for c in configs}
+        best = min(times, key=times.get)
+    with _lock:
+        _cache[key] = best
+    return best
+
+
+def _time_batch_config(precision: int, limiter: int, n: int, ni: bool, config: int,
+                       steps: int) -> float:
+    import torch
+
+    from .batch import BatchSolver, fixed_params
+
+    kw = dict(ohmic=True, hall=True, ambipolar=True, eta_ohm=1e-3, eta_hall=1e-2,
+              eta_ambipolar=1e-3) if ni else {}
+    copies = max(1, min(64, (1 << 22) // (n * n)))
+    b = BatchSolver(precision)
+    try:
+        for i in range(copies):
+            sid = b.add_generated(n, n, _capi.InitSpec.fourier(i), fixed_params(
+                steps + 2, limiter=limiter, **kw), (0, 0), fixed_steps=True)
+            b.set_config(sid, config)
+        b.step(2)  # warm-up: work lists, graph capture
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+    finally:
+        b.close()
+
+
+def tune_batch(precision: int, limiter: int, nx: int, ny: int, ni: bool = False,
+               steps: int = 4, force: bool = False) -> int:
+    """Best batch configuration for this precision, limiter, ideal/non-ideal and size class."""
+    key = "b" + _key(precision, limiter, nx, ny) + f"-n{int(bool(ni))}"
+    with _lock:
+        if not force and key in _cache:
+            return _cache[key]
+    from .batch import batch_configs
+
+    configs = batch_configs(precision)
+    if len(configs) == 1:
+        best = 0
+    else:
+        n = max(16, int(round(math.sqrt(2.0 ** size_class(nx, ny)))))
+        times = {c["config"]: _time_batch_config(precision, limiter, n, ni, c["config"], steps)
                  for c in configs}
         best = min(times, key=times.get)
     with _lock:

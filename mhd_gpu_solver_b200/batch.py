@@ -16,13 +16,29 @@ import numpy as np
 from . import _capi
 
 
+def batch_configs(precision: int) -> list[dict]:
+    """The batch configurations of a precision form: kernel kind, work-item tile, threads."""
+    out = []
+    for c in range(_capi.lib.mhdb_batch_config_count(int(precision))):
+        tx, ty, nt, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _capi.lib.mhdb_batch_config_info(int(precision), c, C.byref(tx), C.byref(ty),
+                                         C.byref(nt), C.byref(kind))
+        out.append({"config": c, "tile_x": tx.value, "tile_y": ty.value, "threads": nt.value,
+                    "kind": _capi.KERNEL_KINDS[kind.value]})
+    return out
+
+
 class BatchSolver:
-    def __init__(self, precision: int = _capi.FP32):
+    """tune=True: each added solve runs the batch configuration the batch autotuner picked for
+    its size class (tuned on first use, cached per process); otherwise the library's default."""
+
+    def __init__(self, precision: int = _capi.FP32, tune: bool = False):
         self._b = C.c_void_p()
         rc = _capi.lib.mhdb_batch_create(int(precision), C.byref(self._b))
         if rc != _capi.OK:
             raise _capi.MhdbError(rc, _capi.lib.mhdb_batch_last_error(None).decode())
         self.precision = int(precision)
+        self.tune = bool(tune)
         self._shapes: dict[int, tuple[int, int, int]] = {}
 
     def _raise(self, rc: int) -> None:
@@ -56,6 +72,7 @@ class BatchSolver:
             _capi.plane_pointers(state), state.shape[1] * state.shape[2], int(bool(fixed_steps)),
             C.byref(sid)))
         self._shapes[sid.value] = state.shape
+        self._tuned(sid.value, nx, ny, params)
         return sid.value
 
     def add_generated(self, nx: int, ny: int, init: "_capi.InitSpec", params: _capi.Params,
@@ -70,7 +87,20 @@ class BatchSolver:
             self._b, C.byref(g), C.byref(params), int(bc[0]), int(bc[1]), C.byref(c),
             int(bool(fixed_steps)), C.byref(sid)))
         self._shapes[sid.value] = (9, int(ny) + 2 * ng, int(nx) + 2 * ng)
+        self._tuned(sid.value, int(nx), int(ny), params)
         return sid.value
+
+    def _tuned(self, sid: int, nx: int, ny: int, params: _capi.Params) -> None:
+        if not self.tune:
+            return
+        from . import autotune
+
+        ni = _capi.nonideal_any(params)
+        self.set_config(sid, autotune.tune_batch(self.precision, params.limiter, nx, ny, ni))
+
+    def set_config(self, sid: int, config: int) -> None:
+        """Run this solve with batch configuration `config` (-1: chosen by its size)."""
+        self._raise(_capi.lib.mhdb_batch_set_config(self._b, int(sid), int(config)))
 
     def remove(self, sid: int) -> None:
         self._raise(_capi.lib.mhdb_batch_remove(self._b, int(sid)))

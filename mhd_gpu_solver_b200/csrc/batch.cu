@@ -5,7 +5,8 @@
 // allocations). Every RK2 step is one persistent launch per stage and per (limiter, non-ideal)
 // combination present: each launch walks a block work-list covering all unfinished solves of that
 // combination (FP64: the shared-memory tile kernel, batch_stage_kernel in stage_kernel.cuh;
-// FP32-mixed: the register strip march, batch_march_kernel in march_kernel.cuh). Each solve
+// FP32-mixed: the TMA strip march, batch_march_tma_kernel in march_tma.cuh, with each solve's
+// tensor maps in its descriptor). Each solve
 // keeps its own Ctrl block (FP64
 // clock, dt, c_h, step count) in one slot array, so one device-to-host copy reports every solve.
 // Chunks of steps are captured as CUDA graphs and replayed while the set of solves is unchanged.
@@ -24,6 +25,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <string>
 #include <utility>
@@ -174,39 +176,77 @@ int blocks_for(long long n, int threads)
     return static_cast<int>(std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 16)));
 }
 
-// Batch kernel pointers of one precision for (limiter, non-ideal, stage), tile config 0.
+// Batch configurations: the kernel variants a solve of a batch can run with (the tile shape, the
+// halo staging and the threads per work item), picked per solve (mhdb_batch_set_config; by
+// default from the solve's size) and so per size class by the batch autotuner.
+struct BatchVariant {
+    int tile_x, tile_y, threads, kind; // kind: MHDB_KERNEL_*
+};
+
 template <class Policy>
 struct BatchKernels;
 
 template <>
 struct BatchKernels<PolicyF64> {
     using Cfg = TileCfg<32, 8, 320, 2>;
-    using Fn = void (*)(const BatchSolve<PolicyF64>*, const int2*, int);
+    using Desc = BatchSolve<PolicyF64>;
+    using Fn = void (*)(const Desc*, const int2*, int);
+    static constexpr int kVariants = 1;
+    static BatchVariant variant(int) { return {Cfg::TX, Cfg::TY, Cfg::NT, MHDB_KERNEL_TILE}; }
+    static int default_variant(long long) { return 0; }
     template <int L, bool NI, int STAGE>
-    static Fn fn() { return batch_stage_kernel<PolicyF64, L, NI, STAGE, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>; }
-    static size_t smem(bool ni) { return ni ? stage_smem_bytes<double, Cfg::TX, Cfg::TY, true>() : stage_smem_bytes<double, Cfg::TX, Cfg::TY, false>(); }
+    static Fn fn(int)
+    {
+        return batch_stage_kernel<PolicyF64, L, NI, STAGE, Cfg::TX, Cfg::TY, Cfg::NT, Cfg::MINB>;
+    }
+    static size_t smem(int, bool ni, int)
+    {
+        return ni ? stage_smem_bytes<double, Cfg::TX, Cfg::TY, true>()
+                  : stage_smem_bytes<double, Cfg::TX, Cfg::TY, false>();
+    }
 };
 
-// FP32-mixed batches run the register strip march (4 warps x 28 columns by 32 rows per block).
+// FP32-mixed variants:
+//   0: TMA strip march, one warp (28 columns x 32 rows) per item, 16 blocks per SM, stage 1
+//      through TMA row stores, stage 2 through plain stores;
+//   1: register strip march (rows loaded by the lanes, no shared-memory staging), 4 warps
+//      (112 columns x 32 rows) per item, 4 blocks per SM;
+//   2: as 0 with 64 rows per item.
 template <>
 struct BatchKernels<PolicyMixed> {
-    struct Cfg {
-        static constexpr int NW = 4, LY = 32, MINB = 4;
-        static constexpr int TX = NW * kMarchOwned, TY = LY, NT = NW * 32;
-    };
-    using Fn = void (*)(const BatchSolve<PolicyMixed>*, const int2*, int);
+    using Desc = BatchSolveTma;
+    using Fn = void (*)(const Desc*, const int2*, int);
+    static constexpr int kVariants = 3;
+    static BatchVariant variant(int v)
+    {
+        if (v == 1) return {4 * kMarchOwned, 32, 128, MHDB_KERNEL_MARCH};
+        if (v == 2) return {kMarchOwned, 64, 32, MHDB_KERNEL_MARCH_TMA};
+        return {kMarchOwned, 32, 32, MHDB_KERNEL_MARCH_TMA};
+    }
+    // Small solves have too few strips to fill the GPU on their own; their per-item set-up is
+    // cheaper in the register march.
+    static int default_variant(long long cells) { return cells >= 128LL * 128 ? 0 : 1; }
     template <int L, bool NI, int STAGE>
-    static Fn fn() { return batch_march_kernel<PolicyMixed, L, NI, STAGE, Cfg::LY, Cfg::NW, Cfg::MINB>; }
-    static size_t smem(bool) { return 0; }
+    static Fn fn(int v)
+    {
+        if (v == 1) return batch_march_kernel<PolicyMixed, L, NI, STAGE, 32, 4, 4, BatchSolveTma>;
+        if (v == 2) return batch_march_tma_kernel<L, NI, STAGE, 64, 1, 16, true, STAGE == 1>;
+        return batch_march_tma_kernel<L, NI, STAGE, 32, 1, 16, true, STAGE == 1>;
+    }
+    static size_t smem(int v, bool, int stage)
+    {
+        if (v == 1) return 0;
+        return stage == 1 ? march_tma_smem_bytes<1, true>(1) : march_tma_smem_bytes<2, false>(1);
+    }
 };
 
 template <class Policy>
-typename BatchKernels<Policy>::Fn batch_fn(int lim, bool ni, int stage)
+typename BatchKernels<Policy>::Fn batch_fn(int variant, int lim, bool ni, int stage)
 {
     using K = BatchKernels<Policy>;
 #define MHDB_BF(LL)                                                                                \
-    if (ni) return stage == 1 ? K::template fn<LL, true, 1>() : K::template fn<LL, true, 2>();     \
-    return stage == 1 ? K::template fn<LL, false, 1>() : K::template fn<LL, false, 2>();
+    if (ni) return stage == 1 ? K::template fn<LL, true, 1>(variant) : K::template fn<LL, true, 2>(variant); \
+    return stage == 1 ? K::template fn<LL, false, 1>(variant) : K::template fn<LL, false, 2>(variant);
     if (lim == kMinmod) {
         MHDB_BF(kMinmod)
     } else if (lim == kMC) {
@@ -229,9 +269,12 @@ struct SolveRec {
     void* Us = nullptr;
     size_t bytes = 0;
     int slot = -1;
+    int config = -1;  // batch configuration chosen for this solve (-1: from its size)
+    int variant = 0;  // configuration in use (set when the work lists are built)
     int tiles_x = 0, tiles_y = 0;
     bool fixed = false;
     Ctrl last{}; // host copy after the last poll
+    MarchTmaMaps maps[2]{}; // FP32-mixed: tensor maps of stage 1 and stage 2
 };
 
 } // namespace
@@ -255,11 +298,12 @@ struct mhdb_batch {
     int ctrl_cap = 0;
     std::vector<int> free_slots;
     int next_slot = 0;
-    void* descs = nullptr;        // device BatchSolve<Policy>[]
+    void* descs = nullptr;        // device descriptors (BatchSolve<PolicyF64> or BatchSolveTma)
     size_t descs_cap = 0;         // bytes
     int2* work = nullptr;
     size_t work_cap = 0;          // items
     struct List {
+        int variant;
         int limiter;
         bool ni;
         int offset, count;
@@ -268,7 +312,7 @@ struct mhdb_batch {
     bool dirty = true;
     size_t bytes_in_use = 0;
     long long launches = 0;
-    int resident_ctas[2][2] = {{0, 0}, {0, 0}}; // [ni][stage-1] CTAs per SM
+    int resident_ctas[4][2][2] = {}; // [variant][ni][stage-1] CTAs per SM
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
 };
@@ -331,15 +375,21 @@ void grow_ctrl(mhdb_batch* b, int need)
 template <class Policy>
 void rebuild(mhdb_batch* b)
 {
-    using Desc = BatchSolve<Policy>;
     using K = BatchKernels<Policy>;
+    using Desc = typename K::Desc;
     std::vector<Desc> descs;
-    std::map<std::pair<int, int>, std::vector<int2>> items;
+    std::map<std::tuple<int, int, int>, std::vector<int2>> items; // (variant, limiter, ni)
     for (size_t id = 0; id < b->solves.size(); ++id) {
         SolveRec& s = b->solves[id];
         if (!s.live || s.last.finished != 0) {
             continue;
         }
+        s.variant = (s.config >= 0 && s.config < K::kVariants)
+                        ? s.config
+                        : K::default_variant(static_cast<long long>(s.grid.nx) * s.grid.ny);
+        const BatchVariant bv = K::variant(s.variant);
+        s.tiles_x = (s.grid.nx + bv.tile_x - 1) / bv.tile_x;
+        s.tiles_y = (s.grid.ny + bv.tile_y - 1) / bv.tile_y;
         Desc d{};
         Ctrl* ctrl = b->ctrl + s.slot;
         if constexpr (sizeof(typename Policy::T) == 8) {
@@ -351,12 +401,14 @@ void rebuild(mhdb_batch* b)
             const MixedState u = mixed_view(s.U, s.geom), us = mixed_view(s.Us, s.geom);
             d.stage[0] = StageArgsMx{u, us, nullptr, ctrl, s.geom, s.k, 1};
             d.stage[1] = StageArgsMx{us, u, nullptr, ctrl, s.geom, s.k, 1};
+            d.maps[0] = s.maps[0];
+            d.maps[1] = s.maps[1];
         }
         d.tiles_x = s.tiles_x;
         d.ntiles = s.tiles_x * s.tiles_y;
         const int di = static_cast<int>(descs.size());
         descs.push_back(d);
-        auto& v = items[{s.limiter, s.ni ? 1 : 0}];
+        auto& v = items[{s.variant, s.limiter, s.ni ? 1 : 0}];
         for (int t = 0; t < d.ntiles; ++t) {
             v.push_back(make_int2(di, t));
         }
@@ -364,7 +416,8 @@ void rebuild(mhdb_batch* b)
     std::vector<int2> work;
     b->lists.clear();
     for (auto& kv : items) {
-        b->lists.push_back({kv.first.first, kv.first.second != 0, static_cast<int>(work.size()),
+        b->lists.push_back({std::get<0>(kv.first), std::get<1>(kv.first),
+                            std::get<2>(kv.first) != 0, static_cast<int>(work.size()),
                             static_cast<int>(kv.second.size())});
         work.insert(work.end(), kv.second.begin(), kv.second.end());
     }
@@ -387,16 +440,17 @@ void rebuild(mhdb_batch* b)
                               cudaMemcpyHostToDevice, b->stream), "cudaMemcpyAsync(work)");
         check(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
     }
-    // CTAs per SM of each kernel family (occupancy of the persistent grid).
-    for (int ni = 0; ni < 2; ++ni) {
+    // CTAs per SM of each kernel family in use (occupancy of the persistent grid).
+    for (const auto& l : b->lists) {
+        const BatchVariant bv = K::variant(l.variant);
         for (int st = 1; st <= 2; ++st) {
-            auto fn = batch_fn<Policy>(kVanLeer, ni != 0, st);
-            const size_t sm = K::smem(ni != 0);
+            auto fn = batch_fn<Policy>(l.variant, l.limiter, l.ni, st);
+            const size_t sm = K::smem(l.variant, l.ni, st);
             check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)),
                   "cudaFuncSetAttribute");
             int nb = 0;
-            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, K::Cfg::NT, sm), "occupancy");
-            b->resident_ctas[ni][st - 1] = std::max(1, nb);
+            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, bv.threads, sm), "occupancy");
+            b->resident_ctas[l.variant][l.ni ? 1 : 0][st - 1] = std::max(1, nb);
         }
     }
     if (b->graph != nullptr) {
@@ -406,19 +460,21 @@ void rebuild(mhdb_batch* b)
     b->dirty = false;
 }
 
+// One RK2 step of every work list: per stage, one persistent launch per list, each filling the
+// GPU with its kernel's resident CTAs.
 template <class Policy>
 void launch_step(mhdb_batch* b, int sms)
 {
     using K = BatchKernels<Policy>;
-    const auto* descs = static_cast<const BatchSolve<Policy>*>(b->descs);
+    const auto* descs = static_cast<const typename K::Desc*>(b->descs);
     for (int stage = 1; stage <= 2; ++stage) {
         for (const auto& l : b->lists) {
-            auto fn = batch_fn<Policy>(l.limiter, l.ni, stage);
-            const size_t sm = K::smem(l.ni);
-            check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)),
-                  "cudaFuncSetAttribute");
-            const int grid = std::min(l.count, sms * b->resident_ctas[l.ni ? 1 : 0][stage - 1]);
-            fn<<<grid, K::Cfg::NT, sm, b->stream>>>(descs, b->work + l.offset, l.count);
+            auto fn = batch_fn<Policy>(l.variant, l.limiter, l.ni, stage);
+            const size_t sm = K::smem(l.variant, l.ni, stage);
+            const int grid =
+                std::min(l.count, sms * b->resident_ctas[l.variant][l.ni ? 1 : 0][stage - 1]);
+            fn<<<grid, K::variant(l.variant).threads, sm, b->stream>>>(descs, b->work + l.offset,
+                                                                      l.count);
             ++b->launches;
         }
     }
@@ -631,10 +687,6 @@ void add_solve(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, 
     s.geom.bc_x = bc_x;
     s.geom.bc_y = bc_y;
     s.geom.plane = static_cast<size_t>(s.geom.pitch) * grid->ny;
-    const int tx = b->precision == MHDB_FP64 ? BatchKernels<PolicyF64>::Cfg::TX : BatchKernels<PolicyMixed>::Cfg::TX;
-    const int ty = b->precision == MHDB_FP64 ? BatchKernels<PolicyF64>::Cfg::TY : BatchKernels<PolicyMixed>::Cfg::TY;
-    s.tiles_x = (grid->nx + tx - 1) / tx;
-    s.tiles_y = (grid->ny + ty - 1) / ty;
     const size_t bytes = 9 * s.geom.plane * 8;
     check(cudaMallocFromPoolAsync(&s.U, bytes, b->pool, b->stream), "cudaMallocFromPoolAsync(U)");
     const cudaError_t e2 = cudaMallocFromPoolAsync(&s.Us, bytes, b->pool, b->stream);
@@ -643,6 +695,16 @@ void add_solve(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, 
         check(e2, "cudaMallocFromPoolAsync(U*)");
     }
     s.bytes = 2 * bytes;
+    if (b->precision != MHDB_FP64) {
+        const MixedState u = mixed_view(s.U, s.geom), us = mixed_view(s.Us, s.geom);
+        std::string err;
+        if (!encode_march_maps(u, us, s.geom, &s.maps[0], &err) ||
+            !encode_march_maps(us, u, s.geom, &s.maps[1], &err)) {
+            cudaFreeAsync(s.U, b->stream);
+            cudaFreeAsync(s.Us, b->stream);
+            throw BatchFail{MHDB_CUDA_ERROR, err};
+        }
+    }
     const long long n = static_cast<long long>(grid->nx) * grid->ny;
     if (comps != nullptr) {
         double* stg = nullptr;
@@ -795,6 +857,43 @@ int mhdb_batch_step(mhdb_batch* b, int nsteps, int* active)
                 n += (s.live && s.last.finished == 0) ? 1 : 0;
             }
             *active = n;
+        }
+    });
+}
+
+int mhdb_batch_config_count(int precision)
+{
+    return precision == MHDB_FP64 ? BatchKernels<PolicyF64>::kVariants
+                                  : BatchKernels<PolicyMixed>::kVariants;
+}
+
+int mhdb_batch_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
+                           int* kind)
+{
+    if (config < 0 || config >= mhdb_batch_config_count(precision)) {
+        return MHDB_INVALID_ARGUMENT;
+    }
+    const BatchVariant v = precision == MHDB_FP64 ? BatchKernels<PolicyF64>::variant(config)
+                                                  : BatchKernels<PolicyMixed>::variant(config);
+    if (tile_x) *tile_x = v.tile_x;
+    if (tile_y) *tile_y = v.tile_y;
+    if (threads) *threads = v.threads;
+    if (kind) *kind = v.kind;
+    return MHDB_OK;
+}
+
+int mhdb_batch_set_config(mhdb_batch* b, int id, int config)
+{
+    return guarded(b, [&] {
+        if (id < 0 || id >= static_cast<int>(b->solves.size()) || !b->solves[id].live) {
+            throw BatchFail{MHDB_INVALID_ARGUMENT, "unknown solve id"};
+        }
+        if (config < -1 || config >= mhdb_batch_config_count(b->precision)) {
+            throw BatchFail{MHDB_INVALID_ARGUMENT, "unknown batch configuration"};
+        }
+        if (b->solves[id].config != config) {
+            b->solves[id].config = config;
+            b->dirty = true;
         }
     });
 }

@@ -206,11 +206,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_kernel(const typename Pol
 }
 
 // Persistent strip-march form over a block work-list of many independent solves (each item:
-// solve index, block index; a block is NW strips of 28 columns by LY rows). Every CTA walks the
+// solve index, block index; a block is NW strips of 28 columns by LY rows; Desc is any
+// descriptor with stage[2], tiles_x and ntiles). Every CTA walks the
 // list with a grid stride, like batch_stage_kernel in stage_kernel.cuh; a solve's signal-speed
 // reduction completes when its last block arrives and that block advances the solve's clock.
-template <class Policy, int L, bool NI, int STAGE, int LY, int NW, int MINB>
-__global__ void __launch_bounds__(NW * 32, MINB) batch_march_kernel(const BatchSolve<Policy>* solves,
+template <class Policy, int L, bool NI, int STAGE, int LY, int NW, int MINB,
+          class Desc = BatchSolve<Policy>>
+__global__ void __launch_bounds__(NW * 32, MINB) batch_march_kernel(const Desc* solves,
                                                                      const int2* __restrict__ work,
                                                                      int nwork)
 {

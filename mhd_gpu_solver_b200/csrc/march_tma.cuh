@@ -48,7 +48,8 @@ constexpr size_t march_tma_smem_bytes(int warps)
 
 template <int L, int STAGE, int LY, bool HF, bool ST, bool NI>
 __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
-                                                  int x0, int y0, int lane, unsigned char* wbase)
+                                                  int x0, int y0, int lane, unsigned char* wbase,
+                                                  bool& failed_out)
 {
     using Policy = PolicyMixed;
     using T = float;
@@ -303,7 +304,8 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
         __syncwarp();
     }
     if (failed) {
-        // Record the failure and let every copy of this warp land before the CTA can exit.
+        // Record the failure and let every copy of this warp land before the CTA can exit; the
+        // caller processes no further strips with these barriers.
         if (lane == 0) {
             atomicOr(&a.ctrl->status, static_cast<int>(kStatusWaitTimeout));
         }
@@ -313,8 +315,17 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
         for (int j = own_done; j < own_issued; ++j) {
             mbar_wait(bar_s + 16 + 8 * (j & 1), static_cast<uint32_t>((j >> 1) & 1));
         }
+        failed_out = true;
         return 0.0;
     }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            mbar_inval(bar_s + 8 * b); // every phase completed; the next strip initialises anew
+        }
+    }
+    __syncwarp();
     return smax;
 }
 
@@ -332,12 +343,76 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArg
     unsigned char* base = march_smem + ((128u - (smem_addr(march_smem) & 127u)) & 127u);
     const int x0 = (blockIdx.x * NW + warp) * kMarchOwned;
     double smax = 0.0;
+    bool failed = false;
     if (x0 < a.geom.nx) { // warp-uniform
-        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
-                                             base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes);
+        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(
+            a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
+            base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes, failed);
     }
     if constexpr (STAGE == 2) {
         reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);
+    }
+}
+
+// One solve of a TMA batch: stage arguments, the tensor maps of both stages, its tiling.
+struct BatchSolveTma {
+    MarchTmaMaps maps[2]; // stage 1 and stage 2
+    StageArgsMx stage[2];
+    int tiles_x; // blocks per row
+    int ntiles;  // blocks of this solve
+};
+
+// Persistent TMA strip march over a block work-list of many independent solves (items: solve
+// index, block index), as batch_march_kernel; the tensor maps come from the descriptor array in
+// global memory (lane 0 acquires them before its copies). A warp whose copies timed out processes
+// no further items (the solve reports kStatusWaitTimeout).
+template <int L, bool NI, int STAGE, int LY, int NW, int MINB, bool HF, bool ST>
+__global__ void __launch_bounds__(NW * 32, MINB) batch_march_tma_kernel(
+    const BatchSolveTma* solves, const int2* __restrict__ work, int nwork)
+{
+    __shared__ __align__(16) StageArgsMx sa;
+    __shared__ int s_tiles_x, s_ntiles;
+    extern __shared__ unsigned char march_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = march_smem + ((128u - (smem_addr(march_smem) & 127u)) & 127u);
+    unsigned char* wbase = base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes;
+    bool failed = false;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 it = work[w];
+        __syncthreads(); // the previous item is done with sa
+        {
+            const int* src = reinterpret_cast<const int*>(&solves[it.x].stage[STAGE - 1]);
+            int* dst = reinterpret_cast<int*>(&sa);
+            for (int i = threadIdx.x; i < static_cast<int>(sizeof(StageArgsMx) / sizeof(int));
+                 i += NW * 32) {
+                dst[i] = src[i];
+            }
+            if (threadIdx.x == 0) {
+                s_tiles_x = solves[it.x].tiles_x;
+                s_ntiles = solves[it.x].ntiles;
+            }
+        }
+        __syncthreads();
+        if (sa.ctrl->finished != 0) {
+            continue;
+        }
+        const MarchTmaMaps& m = solves[it.x].maps[STAGE - 1];
+        const int x0 = ((it.y % s_tiles_x) * NW + warp) * kMarchOwned;
+        const int y0 = (it.y / s_tiles_x) * LY;
+        double smax = 0.0;
+        if (x0 < sa.geom.nx && !failed) { // warp-uniform
+            if (lane == 0) {
+                tensormap_acquire(&m.in_halo);
+                tensormap_acquire(&m.in_own);
+                tensormap_acquire(&m.out_own);
+            }
+            __syncwarp();
+            smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(sa, m, x0, y0, lane, wbase, failed);
+        }
+        if constexpr (STAGE == 2) {
+            reduce_signal_speed_and_finish(smax, sa.ctrl, sa.k, static_cast<unsigned>(s_ntiles),
+                                           true);
+        }
     }
 }
 

@@ -21,7 +21,6 @@
 #include "stage_select.h"
 
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -324,55 +323,6 @@ void validate_params(const mhdb_params* p, bool time_based)
     }
 }
 
-// cuTensorMapEncodeTiled from the driver the runtime is bound to (no link-time libcuda).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        const cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
-                                                               cudaEnableDefault, &q);
-        return (e == cudaSuccess && q == cudaDriverEntryPointSuccess)
-                   ? reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p)
-                   : nullptr;
-    }();
-    if (fn == nullptr) {
-        throw ApiError{MHDB_CUDA_ERROR, "CUDA: cuTensorMapEncodeTiled is not available"};
-    }
-    return fn;
-}
-
-// 3D tensor map (x, y, plane) over the 18 float planes of a mixed state: extent nx x ny x 18,
-// row stride pitch floats, plane stride g.plane floats; elements outside the extent read as 0.
-CUtensorMap mixed_tensor_map(const MixedState& s, const Geometry& g, unsigned box_x,
-                             unsigned box_planes)
-{
-    CUtensorMap map;
-    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.nx), static_cast<cuuint64_t>(g.ny), 18};
-    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float),
-                                   static_cast<cuuint64_t>(g.plane) * sizeof(float)};
-    const cuuint32_t box[3] = {box_x, 1, box_planes};
-    const cuuint32_t elem[3] = {1, 1, 1};
-    const CUresult r = tensor_map_encoder()(
-        &map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, s.hi, dims, strides, box, elem,
-        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-        throw ApiError{MHDB_CUDA_ERROR, "CUDA: cuTensorMapEncodeTiled failed (" +
-                                            std::to_string(static_cast<int>(r)) + ")"};
-    }
-    return map;
-}
-
-MarchTmaMaps march_maps(const MixedState& in, const MixedState& out, const Geometry& g)
-{
-    MarchTmaMaps m;
-    m.in_halo = mixed_tensor_map(in, g, kTmaHaloW, 9);
-    m.in_own = mixed_tensor_map(in, g, kTmaOwnW, 18);
-    m.out_own = mixed_tensor_map(out, g, kTmaOwnW, 18);
-    return m;
-}
-
 // Launch plan of one RK2 step for the current state and parameters.
 struct StepPlan {
     bool mixed = false;
@@ -425,8 +375,11 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
         if (sk.mx_tma1 != nullptr) {
             s.t1 = sk.mx_tma1;
             s.t2 = sk.mx_tma2;
-            s.tm1 = march_maps(u, us, h->geom);
-            s.tm2 = march_maps(us, u, h->geom);
+            std::string err;
+            if (!encode_march_maps(u, us, h->geom, &s.tm1, &err) ||
+                !encode_march_maps(us, u, h->geom, &s.tm2, &err)) {
+                throw ApiError{MHDB_CUDA_ERROR, err};
+            }
         }
     }
     if (sk.threads == 0) {

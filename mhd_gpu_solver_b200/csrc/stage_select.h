@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cstddef>
+#include <string>
 
 #include "stage_f64.cuh"
 #include "stage_mixed.cuh"
@@ -42,6 +43,11 @@ TileConfigInfo stage_config_info_mixed(int config);
 
 // Kernels of one configuration; config != 0 is available only for ideal, unmasked solves
 // (threads == 0 otherwise).
+// Tensor maps of one TMA strip-march stage reading `in` and writing `out` (tma_maps.cu); false
+// with a message when the driver cannot encode them.
+bool encode_march_maps(const MixedState& in, const MixedState& out, const Geometry& g,
+                       MarchTmaMaps* maps, std::string* err);
+
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);
 

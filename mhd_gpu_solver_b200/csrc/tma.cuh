@@ -38,6 +38,19 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
+// Ends an mbarrier's life (before its shared memory is initialised as a new one).
+__device__ __forceinline__ void mbar_inval(uint32_t bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Orders earlier generic-proxy writes of a tensor map in global memory (the host's copy of the
+// batch descriptors) before this thread's TMA copies through it.
+__device__ __forceinline__ void tensormap_acquire(const void* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
 // Makes mbarrier initialisation visible to the async proxy (the TMA unit).
 __device__ __forceinline__ void fence_mbar_init()
 {

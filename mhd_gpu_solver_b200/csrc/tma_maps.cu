@@ -1,0 +1,65 @@
+// Host side of the TMA strip march: tensor maps of a mixed state, encoded with the driver's
+// cuTensorMapEncodeTiled (looked up through the runtime, so the library does not link libcuda).
+#include "stage_select.h"
+
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <string>
+
+namespace mhdb {
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        const cudaError_t e = cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
+                                                               cudaEnableDefault, &q);
+        return (e == cudaSuccess && q == cudaDriverEntryPointSuccess)
+                   ? reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p)
+                   : nullptr;
+    }();
+    return fn;
+}
+
+// 3D tensor map (x, y, plane) over the 18 float planes of a mixed state: extent nx x ny x 18,
+// row stride pitch floats, plane stride g.plane floats; elements outside the extent read as 0
+// and are not written.
+bool mixed_tensor_map(const MixedState& s, const Geometry& g, unsigned box_x, unsigned box_planes,
+                      CUtensorMap* map, std::string* err)
+{
+    auto encode = tensor_map_encoder();
+    if (encode == nullptr) {
+        *err = "CUDA: cuTensorMapEncodeTiled is not available";
+        return false;
+    }
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(g.nx), static_cast<cuuint64_t>(g.ny), 18};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(g.pitch) * sizeof(float),
+                                   static_cast<cuuint64_t>(g.plane) * sizeof(float)};
+    const cuuint32_t box[3] = {box_x, 1, box_planes};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, s.hi, dims, strides, box,
+                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        *err = "CUDA: cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")";
+        return false;
+    }
+    return true;
+}
+
+} // namespace
+
+bool encode_march_maps(const MixedState& in, const MixedState& out, const Geometry& g,
+                       MarchTmaMaps* maps, std::string* err)
+{
+    return mixed_tensor_map(in, g, kTmaHaloW, 9, &maps->in_halo, err) &&
+           mixed_tensor_map(in, g, kTmaOwnW, 18, &maps->in_own, err) &&
+           mixed_tensor_map(out, g, kTmaOwnW, 18, &maps->out_own, err);
+}
+
+} // namespace mhdb

@@ -141,10 +141,26 @@ class ServeStats:
                 "chunks": self.chunks}
 
 
+def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
+    """Tune the batch configuration of every size class the requests fall into (the batch
+    autotuner caches its choices per process), so that serving does not tune on admission."""
+    from . import autotune
+
+    seen = set()
+    for req in requests:
+        ni = _capi.nonideal_any(req.params())
+        key = (req.limiter, ni, autotune.size_class(req.n, req.n))
+        if key not in seen:
+            seen.add(key)
+            autotune.tune_batch(precision, req.limiter, req.n, req.n, ni)
+
+
 def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
-          chunk: int = 16, download: bool = True, keep_states: bool = False) -> ServeStats:
-    """Serve a request stream in real time with continuous batching."""
-    batch = BatchSolver(precision)
+          chunk: int = 16, download: bool = True, keep_states: bool = False,
+          tune: bool = True) -> ServeStats:
+    """Serve a request stream in real time with continuous batching. tune: each request runs
+    the batch configuration tuned for its size class (see prepare)."""
+    batch = BatchSolver(precision, tune=tune)
     stats = ServeStats()
     results = ResultBuffer()
     pending = deque(sorted(requests, key=lambda r: r.arrival))

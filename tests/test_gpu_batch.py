@@ -210,3 +210,43 @@ def test_launch_poll_and_downloads_beside_running_steps():
     b.close()
     for sid, ref in zip(ids, refs):
         assert np.array_equal(got[sid], ref)
+
+
+def test_every_batch_configuration_gives_the_same_values():
+    """The FP32-mixed batch configurations (TMA strip march with 32- or 64-row items, register
+    strip march) run the same arithmetic and agree to FP32 rounding (the compiler may contract
+    the non-ideal products differently in the segment prologue and the row loop), and match the
+    FP64 batch within the FP32-mixed tolerance, ideal and non-ideal."""
+    from mhd_gpu_solver_b200 import autotune
+    from mhd_gpu_solver_b200.batch import batch_configs
+
+    cases = [CASES[0], CASES[1], CASES[3], CASES[4], CASES[5]]
+    states = [state(c[0], c[1], 60 + i, c[2], c[3], c[6]) for i, c in enumerate(cases)]
+    configs = batch_configs(_capi.FP32)
+    assert {c["kind"] for c in configs} >= {"march", "march_tma"}
+    outs = []
+    for cfg in configs:
+        b = BatchSolver(_capi.FP32)
+        ids = []
+        for U, c in zip(states, cases):
+            sid = b.add(U, fixed_params(20, **params_of(c)), c[3], fixed_steps=True)
+            b.set_config(sid, cfg["config"])
+            ids.append(sid)
+        assert b.step(20) == 0
+        outs.append([b.download(i) for i in ids])
+        b.close()
+    for cfg, other in zip(configs[1:], outs[1:]):
+        for a, c in zip(outs[0], other):
+            assert np.all(rel_l1(c, a)[[0, 1, 2, 4, 5, 6]] <= 1e-6), cfg
+    b64 = BatchSolver(_capi.FP64)
+    ids = [b64.add(U, fixed_params(20, **params_of(c)), c[3], fixed_steps=True)
+           for U, c in zip(states, cases)]
+    b64.step(20)
+    for sid, got in zip(ids, outs[0]):
+        err = rel_l1(got, b64.download(sid))
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= 1e-6), err
+    b64.close()
+    best = autotune.tune_batch(_capi.FP32, _capi.VANLEER, 100, 100, False, steps=2)
+    assert 0 <= best < len(configs)
+    with pytest.raises(ValueError):
+        BatchSolver(_capi.FP32).set_config(0, 0)  # unknown solve id
