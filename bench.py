@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--batch-solves", type=int, default=256,
                     help="solves of the batched workload (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--masked-steps", type=int, default=300,
+                    help="RK2 steps of the masked non-ideal 2048^2 leg (0 skips it)")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests of the served stream (0 skips it)")
     ap.add_argument("--serve-side", default="128,1024")
@@ -307,6 +309,59 @@ def bench_batched(nsolves: int, steps: int, seed: int = 1) -> dict:
             "gpu_launches": launches}
 
 
+def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
+    """The non-ideal, masked workload: n^2, the seeded Fourier state (generated on the device),
+    Ohmic 1e-3, Hall 1e-2, ambipolar 1e-3, 12 circles and 6 rectangles of reflective walls,
+    outflow in x and periodic in y, van Leer, `steps` RK2 steps, FP64 plain vs FP32-mixed (both
+    on the shared-memory tile kernel, the masked path). Reports each form's zone-updates/s, the
+    FP32-mixed L1 error against the FP64 result, and the FP64 div-B norms and mass/energy
+    drift."""
+    import torch
+
+    from mhd_gpu_solver_b200 import _capi
+    from mhd_gpu_solver_b200 import workloads as wl
+
+    mask = wl.circles_and_rectangles(n, n, seed)
+    params = _capi.make_params(limiter=_capi.VANLEER, ohmic=True, hall=True, ambipolar=True,
+                               eta_ohm=1e-3, eta_hall=1e-2, eta_ambipolar=1e-3)
+    out, states = {}, {}
+    for name, prec in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32)):
+        dev = _capi.DeviceSolver(n, n, precision=prec)
+        try:
+            dev.configure(_capi.BC_OUTFLOW, _capi.BC_PERIODIC, mask, True)
+            dev.generate(_capi.InitSpec.fourier(seed), params)
+            d0 = dev.diagnostics(params)
+            dev.solve_steps(params, 2)  # warm-up (kernel attributes, graph capture)
+            dev.generate(_capi.InitSpec.fourier(seed), params)
+            stream = torch.cuda.ExternalStream(dev.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r = dev.solve_steps(params, steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            d1 = dev.diagnostics(params)
+            states[name] = dev.download()
+        finally:
+            dev.close()
+        out[name] = {"zone_updates_per_s": float(n) * n * steps / (ms * 1e-3), "ms": ms,
+                     "steps": r.steps, "t": r.t,
+                     "div_b_l2": d1["div_b_l2"], "div_b_max": d1["div_b_max"],
+                     "mass_drift": (d1["mass"] - d0["mass"]) / d0["mass"],
+                     "energy_drift": (d1["energy"] - d0["energy"]) / d0["energy"]}
+    inner = (slice(None), slice(2, -2), slice(2, -2))
+    a, b = states["fp32_mixed"][inner], states["fp64"][inner]
+    num = np.abs(a - b).reshape(9, -1).sum(axis=1)
+    den = np.abs(b).reshape(9, -1).sum(axis=1)
+    l1 = num / np.where(den > 0, den, 1.0)
+    out["workload"] = (f"{n}^2 masked (12 circles, 6 rectangles, reflective walls), Ohmic/Hall/"
+                       f"ambipolar 1e-3/1e-2/1e-3, outflow x, periodic y, van Leer, {steps} steps")
+    out["speedup_fp32_mixed_over_fp64"] = out["fp64"]["ms"] / out["fp32_mixed"]["ms"]
+    out["l1_fp32_mixed_vs_fp64_max"] = float(np.max(l1[[0, 1, 2, 4, 5, 6]]))
+    return out
+
+
 def bench_served(nreq: int, side, tend) -> dict:
     from mhd_gpu_solver_b200.serve import make_stream, prepare, serve, serve_one_at_a_time
 
@@ -484,6 +539,8 @@ def main():
     }
     if rank == 0 and args.batch_solves > 0:
         line["batched"] = bench_batched(args.batch_solves, args.batch_steps)
+    if rank == 0 and args.masked_steps > 0:
+        line["masked_nonideal"] = bench_masked_nonideal(2048, args.masked_steps)
     if rank == 0 and args.serve_requests > 0:
         side = tuple(int(v) for v in args.serve_side.split(","))
         tend = tuple(float(v) for v in args.serve_tend.split(","))
