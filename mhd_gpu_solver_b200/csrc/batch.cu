@@ -230,13 +230,13 @@ struct BatchKernels<PolicyMixed> {
     static Fn fn(int v)
     {
         if (v == 1) return batch_march_kernel<PolicyMixed, L, NI, STAGE, 32, 4, 4, BatchSolveTma>;
-        if (v == 2) return batch_march_tma_kernel<L, NI, STAGE, 64, 1, 16, true, STAGE == 1>;
-        return batch_march_tma_kernel<L, NI, STAGE, 32, 1, 16, true, STAGE == 1>;
+        if (v == 2) return batch_march_tma_kernel<L, NI, STAGE, 64, 1, 16, true, (STAGE == 1 ? 1 : 0)>;
+        return batch_march_tma_kernel<L, NI, STAGE, 32, 1, 16, true, (STAGE == 1 ? 1 : 0)>;
     }
     static size_t smem(int v, bool, int stage)
     {
         if (v == 1) return 0;
-        return stage == 1 ? march_tma_smem_bytes<1, true>(1) : march_tma_smem_bytes<2, false>(1);
+        return stage == 1 ? march_tma_smem_bytes<1, 1>(1) : march_tma_smem_bytes<2, 0>(1);
     }
 };
 

@@ -45,12 +45,12 @@ struct MarchCfg {
 
 // TMA-fed strip-march configuration (FP32-mixed form only): NW warps per block, LY rows per
 // warp, MINB blocks per SM.
-template <int NW_, int LY_, int MINB_, bool HF_ = true, bool ST1_ = true, bool ST2_ = false>
+template <int NW_, int LY_, int MINB_, bool HF_ = true, int ST1_ = 1, int ST2_ = 0>
 struct MarchTmaCfg {
     static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
-    static constexpr bool HF = HF_;   // wait for the halo row before the x sweep
-    static constexpr bool ST1 = ST1_; // stage 1 results leave through TMA row stores
-    static constexpr bool ST2 = ST2_; // the same for stage 2
+    static constexpr bool HF = HF_; // wait for the halo row before the x sweep
+    static constexpr int ST1 = ST1_; // stage 1: 0 lane stores, 1 or 2 staging slots of TMA stores
+    static constexpr int ST2 = ST2_; // the same for stage 2
     static constexpr bool MARCH_TMA = true;
 };
 

@@ -14,8 +14,8 @@ using Cfg6 = MarchCfg<4, 64, 3>;
 using Cfg7 = MarchTmaCfg<4, 32, 4>;
 using Cfg8 = MarchTmaCfg<2, 32, 8>;
 using Cfg9 = MarchTmaCfg<1, 32, 16>;
-using Cfg10 = MarchTmaCfg<4, 32, 4, true, false>;
-using Cfg11 = MarchTmaCfg<1, 32, 16, true, false>;
+using Cfg10 = MarchTmaCfg<4, 32, 4, true, 0>;
+using Cfg11 = MarchTmaCfg<1, 32, 16, true, 0>;
 using Cfg12 = MarchTmaCfg<1, 64, 16>;
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},

@@ -23,9 +23,10 @@
 
 namespace mhdb {
 
-// Shared memory of one warp: 2 halo slots, 2 own slots, (ST) one staging slot for the row store,
+// Shared memory of one warp: 2 halo slots, 2 own slots, ST staging slots for the row stores
+// (ST = 0: results are stored by the lanes; 1 or 2: TMA row stores through 1 or 2 staging slots),
 // then the 4 mbarriers.
-template <int STAGE, bool ST>
+template <int STAGE, int ST>
 struct MarchTmaLayout {
     static constexpr int kHaloFloats = 9 * kTmaHaloW;             // 324 floats, 1296 B
     static constexpr int kHaloBytes = kHaloFloats * 4;
@@ -36,17 +37,17 @@ struct MarchTmaLayout {
     static constexpr int kOwnSlot = kOwnBoxes * kOwnBoxSlot;
     static constexpr int kOwnTx = kOwnBoxes * kOwnBoxBytes;       // transaction bytes per row
     static constexpr int kStageOff = 2 * kHaloSlot + 2 * kOwnSlot;
-    static constexpr int kBarOff = kStageOff + (ST ? kOwnBoxSlot : 0);
+    static constexpr int kBarOff = kStageOff + ST * kOwnBoxSlot;
     static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
 };
 
-template <int STAGE, bool ST>
+template <int STAGE, int ST>
 constexpr size_t march_tma_smem_bytes(int warps)
 {
     return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST>::kWarpBytes + 128;
 }
 
-template <int L, int STAGE, int LY, bool HF, bool ST, bool NI>
+template <int L, int STAGE, int LY, bool HF, int ST, bool NI>
 __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
                                                   int x0, int y0, int lane, unsigned char* wbase,
                                                   bool& failed_out)
@@ -237,9 +238,9 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 break;
             }
             own_done = i + 1;
-            if constexpr (ST) {
+            if constexpr (ST > 0) {
                 if (lane == 0) {
-                    bulk_wait_read_all(); // the store of row y - 1 has read the staging slot
+                    bulk_wait_read<ST - 1>(); // the store that last used this slot has read it
                 }
                 __syncwarp();
             }
@@ -257,8 +258,8 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                     return q < 18 ? src[q * kTmaOwnW]
                                   : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
                 };
-                if constexpr (ST) {
-                    float* dst = stg_f + (lane - 2);
+                if constexpr (ST > 0) {
+                    float* dst = stg_f + (i % (ST > 0 ? ST : 1)) * (Lay::kOwnBoxSlot / 4) + (lane - 2);
                     Policy::template update_ops<STAGE>(a, false, Lc, dt, k, smax, op,
                                                        [&](int c, float h, float l) {
                                                            dst[c * kTmaOwnW] = h;
@@ -271,8 +272,10 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             }
             __syncwarp();
             if (lane == 0) {
-                if constexpr (ST) {
-                    tma_store_3d(&m.out_own, stg_s, x0, y, 0);
+                if constexpr (ST > 0) {
+                    tma_store_3d(&m.out_own,
+                                 stg_s + static_cast<uint32_t>(i % (ST > 0 ? ST : 1)) * Lay::kOwnBoxSlot,
+                                 x0, y, 0);
                     bulk_commit();
                 }
                 if (i + 2 < nrows) {
@@ -297,7 +300,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             }
         }
     }
-    if constexpr (ST) {
+    if constexpr (ST > 0) {
         if (lane == 0) {
             bulk_wait_all(); // the row stores have written global memory and read their source
         }
@@ -329,7 +332,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     return smax;
 }
 
-template <int L, int STAGE, int LY, int NW, int MINB, bool HF, bool ST, bool NI>
+template <int L, int STAGE, int LY, int NW, int MINB, bool HF, int ST, bool NI>
 __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArgsMx a,
                                                                    const __grid_constant__ MarchTmaMaps m)
 {
@@ -366,7 +369,7 @@ struct BatchSolveTma {
 // index, block index), as batch_march_kernel; the tensor maps come from the descriptor array in
 // global memory (lane 0 acquires them before its copies). A warp whose copies timed out processes
 // no further items (the solve reports kStatusWaitTimeout).
-template <int L, bool NI, int STAGE, int LY, int NW, int MINB, bool HF, bool ST>
+template <int L, bool NI, int STAGE, int LY, int NW, int MINB, bool HF, int ST>
 __global__ void __launch_bounds__(NW * 32, MINB) batch_march_tma_kernel(
     const BatchSolveTma* solves, const int2* __restrict__ work, int nwork)
 {

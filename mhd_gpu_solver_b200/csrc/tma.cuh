@@ -130,10 +130,12 @@ __device__ __forceinline__ void bulk_commit()
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 
-// All committed bulk stores of this thread have finished reading their shared-memory source.
-__device__ __forceinline__ void bulk_wait_read_all()
+// All but the N most recent committed bulk stores of this thread have finished reading their
+// shared-memory source.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
 {
-    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
 }
 
 // All committed bulk stores of this thread are complete (their global writes performed).
