@@ -170,6 +170,9 @@ int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);
 int mhdb_tile_config_kind(int precision, int config);
+/* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves without a mask of at
+   least 1024 x 1024 cells run the TMA strip march (one warp per block), every other solve
+   configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
 /* ---------------------------------------------------------------- batched form (additive)

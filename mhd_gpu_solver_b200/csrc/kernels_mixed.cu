@@ -30,6 +30,11 @@ constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 
 int stage_config_count_mixed() { return kCount; }
 
+// Without a chosen configuration: unmasked grids of at least 1024^2 cells run the TMA strip march
+// with one warp per block (configuration 9); smaller grids have too few 28-column strips to fill
+// the GPU with it and run the shared-memory tile kernel.
+int default_stage_config_mixed(long long cells) { return cells >= 1024LL * 1024 ? 9 : 0; }
+
 TileConfigInfo stage_config_info_mixed(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }
 
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config)

@@ -231,7 +231,7 @@ struct mhdb_solver {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<double> graph_key;
 
-    int tile_config = 0; // index into the compiled tile configurations (0 = default)
+    int tile_config = -1; // index into the compiled tile configurations (-1: by grid size)
     bool profiling = false;
     std::vector<Prof> prof_pending;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pool;
@@ -345,7 +345,13 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     StageKernels sk{};
     // Tuned configurations serve unmasked solves (the tile ones other than 0 ideal solves only,
     // the strip-march ones non-ideal solves too); every other solve uses configuration 0.
-    int cfg = h->has_mask ? 0 : h->tile_config;
+    const long long cells = static_cast<long long>(h->grid.nx) * h->grid.ny;
+    int cfg = h->tile_config >= 0 ? h->tile_config
+                                  : (h->precision == MHDB_FP64 ? default_stage_config_f64(cells)
+                                                               : default_stage_config_mixed(cells));
+    if (h->has_mask) {
+        cfg = 0;
+    }
     if (cfg != 0 && (h->precision == MHDB_FP64 ? select_stage_f64(p->limiter, ni, false, cfg)
                                                : select_stage_mixed(p->limiter, ni, false, cfg))
                             .threads == 0) {
@@ -1044,7 +1050,7 @@ int mhdb_set_tile_config(mhdb_solver* h, int config)
     if (h == nullptr) {
         return MHDB_INVALID_ARGUMENT;
     }
-    if (config < 0 || config >= mhdb_tile_config_count(h->precision)) {
+    if (config < -1 || config >= mhdb_tile_config_count(h->precision)) {
         h->last_error = "unknown tile configuration";
         return MHDB_INVALID_ARGUMENT;
     }

@@ -38,6 +38,9 @@ struct TileConfigInfo {
 // Number of tile configurations compiled per precision form, and their shapes.
 int stage_config_count_f64();
 int stage_config_count_mixed();
+// Configuration used when none is chosen (mhdb_set_tile_config(h, -1), the default).
+int default_stage_config_f64(long long cells);
+int default_stage_config_mixed(long long cells);
 TileConfigInfo stage_config_info_f64(int config);
 TileConfigInfo stage_config_info_mixed(int config);
 

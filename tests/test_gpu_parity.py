@@ -394,3 +394,24 @@ def test_nonideal_strip_march_configurations_match_oracle(precision, case):
         assert abs(r.t - tr) <= (1e-12 if precision == _capi.FP64 else 1e-6) * max(1.0, tr)
         err = rel_l1(got, ref)
         assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (cfg, err)
+
+
+def test_default_configuration_of_a_large_grid_matches_fp64():
+    """Without a chosen configuration a 1024^2 FP32-mixed solve runs the TMA strip march (the
+    drop-in's default for large unmasked grids); it stays within the FP32-mixed tolerance of the
+    FP64 form, ideal and non-ideal."""
+    n = 1024
+    U0 = initial_state(wl.fourier_state(n, n, 2), 5.0 / 3.0)
+    for kw in ({}, NI_PARAMS):
+        outs = {}
+        for prec in (_capi.FP64, _capi.FP32):
+            dev = _capi.DeviceSolver(n, n, precision=prec)
+            dev.configure(0, 0)
+            dev.upload(U0)
+            r = dev.solve_steps(_capi.make_params(limiter=_capi.VANLEER, **kw), 6)
+            outs[prec] = (dev.download(), r)
+            dev.close()
+        (u64, r64), (u32, r32) = outs[_capi.FP64], outs[_capi.FP32]
+        assert r32.steps == r64.steps == 6
+        err = rel_l1(u32, u64)
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (kw, err)
