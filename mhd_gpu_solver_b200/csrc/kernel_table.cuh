@@ -128,7 +128,7 @@ StageKernels select_full(int lim, bool ni, bool mask)
 // Tuning configurations: unmasked solves; the shared-memory tile configurations other than the
 // default serve ideal solves only, the strip-march ones ideal and non-ideal solves.
 template <class Policy, class Cfg>
-StageKernels select_ideal(int lim, bool ni, bool mask)
+StageKernels select_unmasked(int lim, bool ni, bool mask)
 {
     StageKernels k;
     if (mask) {

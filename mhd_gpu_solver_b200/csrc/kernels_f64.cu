@@ -27,15 +27,15 @@ StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config)
 {
     switch (config) {
     case 1:
-        return select_ideal<PolicyF64, Cfg1>(limiter, nonideal, mask);
+        return select_unmasked<PolicyF64, Cfg1>(limiter, nonideal, mask);
     case 2:
-        return select_ideal<PolicyF64, Cfg2>(limiter, nonideal, mask);
+        return select_unmasked<PolicyF64, Cfg2>(limiter, nonideal, mask);
     case 3:
-        return select_ideal<PolicyF64, Cfg3>(limiter, nonideal, mask);
+        return select_unmasked<PolicyF64, Cfg3>(limiter, nonideal, mask);
     case 4:
-        return select_ideal<PolicyF64, Cfg4>(limiter, nonideal, mask);
+        return select_unmasked<PolicyF64, Cfg4>(limiter, nonideal, mask);
     case 5:
-        return select_ideal<PolicyF64, Cfg5>(limiter, nonideal, mask);
+        return select_unmasked<PolicyF64, Cfg5>(limiter, nonideal, mask);
     default:
         return select_full<PolicyF64, Cfg0>(limiter, nonideal, mask);
     }

@@ -41,29 +41,29 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
 {
     switch (config) {
     case 1:
-        return select_ideal<PolicyMixed, Cfg1>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg1>(limiter, nonideal, mask);
     case 2:
-        return select_ideal<PolicyMixed, Cfg2>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg2>(limiter, nonideal, mask);
     case 3:
-        return select_ideal<PolicyMixed, Cfg3>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg3>(limiter, nonideal, mask);
     case 4:
-        return select_ideal<PolicyMixed, Cfg4>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg4>(limiter, nonideal, mask);
     case 5:
-        return select_ideal<PolicyMixed, Cfg5>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg5>(limiter, nonideal, mask);
     case 6:
-        return select_ideal<PolicyMixed, Cfg6>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg6>(limiter, nonideal, mask);
     case 7:
-        return select_ideal<PolicyMixed, Cfg7>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg7>(limiter, nonideal, mask);
     case 8:
-        return select_ideal<PolicyMixed, Cfg8>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg8>(limiter, nonideal, mask);
     case 9:
-        return select_ideal<PolicyMixed, Cfg9>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg9>(limiter, nonideal, mask);
     case 10:
-        return select_ideal<PolicyMixed, Cfg10>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg10>(limiter, nonideal, mask);
     case 11:
-        return select_ideal<PolicyMixed, Cfg11>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg11>(limiter, nonideal, mask);
     case 12:
-        return select_ideal<PolicyMixed, Cfg12>(limiter, nonideal, mask);
+        return select_unmasked<PolicyMixed, Cfg12>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }
