@@ -136,6 +136,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_device(world: int, local: int, visible: str | None):
+    """(physical GPU index for nvidia-smi, CUDA_VISIBLE_DEVICES to set or None, device index to
+    use). One GPU per process: with several ranks each process sees only its own GPU, so the CUDA
+    runtime linked into libmhd_b200.so and torch's runtime both address it as device 0."""
+    if world <= 1:
+        return local, None, local
+    ids = visible.split(",") if visible else [str(i) for i in range(local + 1)]
+    mine = ids[local].strip()
+    return (int(mine) if mine.isdigit() else local), mine, 0
+
+
 def max_over_ranks(ms: float, dist=None) -> float:
     """Slowest rank's device time (ms): the whole-job time of a replicas run."""
     if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
@@ -446,7 +457,10 @@ def main():
 
     import torch
 
-    torch.cuda.set_device(local)
+    phys, visible, index = rank_device(world, local, os.environ.get("CUDA_VISIBLE_DEVICES"))
+    if visible is not None:
+        os.environ["CUDA_VISIBLE_DEVICES"] = visible
+    torch.cuda.set_device(index)
     dist = None
     if world > 1:
         import datetime
@@ -483,7 +497,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         if name == "fp32_mixed":
-            with ClockSampler(local) as clk:
+            with ClockSampler(phys) as clk:
                 r = time_form(dev, params, args.steps, args.warmup, n)
             r["clocks"] = clk.summary()
         else:

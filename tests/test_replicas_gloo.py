@@ -56,3 +56,11 @@ def test_single_process_aggregation():
 
     assert bench.max_over_ranks(3.5, None) == 3.5
     assert bench.replicas_value(100.0, 1000.0, 1) == 100.0
+
+
+def test_each_rank_sees_only_its_own_gpu():
+    import bench
+
+    assert bench.rank_device(1, 0, None) == (0, None, 0)
+    assert bench.rank_device(4, 2, None) == (2, "2", 0)
+    assert bench.rank_device(2, 1, "4,5") == (5, "5", 0)
