@@ -536,6 +536,15 @@ typedef struct {
     double* fy;   /* 9 planes of (ny + 1) x nx */
 } work_t;
 
+void mhdo_nonideal_e(const double* J, const double* B, const mhdo_params* p, double* E)
+{
+    vec3 j = {J[0], J[1], J[2]}, b = {B[0], B[1], B[2]};
+    const vec3 e = nonideal_e(j, b, p);
+    E[0] = e.x;
+    E[1] = e.y;
+    E[2] = e.z;
+}
+
 static int work_alloc(const geom* G, work_t* w)
 {
     const size_t nfx = (size_t)G->ny * (size_t)(G->nx + 1);

@@ -80,6 +80,10 @@ int mhdo_cfl(const mhdo_grid* g, const mhdo_params* p, const uint8_t* mask, cons
 /* Slope limiter phi(a, b) (muscl_hll.hpp:33-57, plus van Leer). */
 double mhdo_limiter(int kind, double a, double b);
 
+/* Generalised Ohm's law E(J, B) of the non-ideal terms enabled in p (include/mhd/nonideal.hpp:
+   63-102). */
+void mhdo_nonideal_e(const double* J, const double* B, const mhdo_params* p, double* E);
+
 /* Face flux from a 4-cell primitive stencil, x-frame order
    (rho, vn, vt, vz, p, bn, bt, bz, psi); out is the rotated-frame flux
    (rho, mn, mt, mz, E, bn, bt, bz, psi) (muscl_hll.hpp:126-209). */

@@ -141,6 +141,8 @@ def _lib(impl: str) -> C.CDLL:
         lib.mhdo_apply_bc.argtypes = [C.POINTER(_Grid), C.c_int, C.c_int, _PD]
         lib.mhdo_wall_fill.argtypes = [C.POINTER(_Grid), _PU8, C.c_double, _PD]
         lib.mhdo_cfl.argtypes = [C.POINTER(_Grid), C.POINTER(_Params), _PU8, _PD, _PD, _PD]
+        lib.mhdo_nonideal_e.argtypes = [_PD, _PD, C.POINTER(_Params), _PD]
+        lib.mhdo_nonideal_e.restype = None
         lib.mhdo_limiter.argtypes = [C.c_int, C.c_double, C.c_double]
         lib.mhdo_limiter.restype = C.c_double
         lib.mhdo_face_flux.argtypes = [C.c_int, _PD, _PD, _PD, _PD, C.c_double, C.c_double, _PD]
@@ -227,6 +229,16 @@ def cfl(U: np.ndarray, grid: Grid, params: Params, mask=None) -> tuple[float, fl
 
 def limiter(kind: int, a: float, b: float) -> float:
     return _lib("oracle").mhdo_limiter(int(kind), float(a), float(b))
+
+
+def nonideal_e(J, B, params: Params) -> np.ndarray:
+    """E = eta_O J + eta_H J x B / |B| + eta_A (J x B) x B / |B|^2 of the enabled terms."""
+    j = np.ascontiguousarray(J, dtype=np.float64)
+    b = np.ascontiguousarray(B, dtype=np.float64)
+    e = np.zeros(3)
+    p = params.c()
+    _lib("oracle").mhdo_nonideal_e(_pd(j), _pd(b), C.byref(p), _pd(e))
+    return e
 
 
 def face_flux(kind: int, wmm, wm, w0, wp, gamma: float, c_h: float) -> np.ndarray:
