@@ -155,15 +155,16 @@ int mhdb_profile_read(mhdb_solver* h, double* ms_stage1, int* n_stage1, double* 
 /* Additive: number of kernel launches this handle has issued (graph nodes included). */
 long long mhdb_launch_count(const mhdb_solver* h);
 
-/* Additive: tile configurations of the stage kernels. Configuration 0 (the default) serves every
-   solve; the others serve solves without a mask (the strip-march ones ideal and non-ideal solves,
-   the other tile ones ideal solves only; a solve they do not serve runs configuration 0) and are
-   picked per grid size class by the autotuner (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells
-   one CTA covers (tile width and height), threads per CTA and the minimum CTAs per SM of one
-   configuration; mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile,
-   separate x and y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp
-   strip march, 28 columns per warp) or MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk
-   copies into shared memory; FP32-mixed only), or -1 for an unknown configuration. */
+/* Additive: tile configurations of the stage kernels. Configuration 0 (the shared-memory tile
+   kernel) serves every solve; the others serve solves without a mask (the strip-march ones ideal
+   and non-ideal solves, the other tile ones ideal solves only; a solve they do not serve runs
+   configuration 0) and are picked per grid size class by the autotuner
+   (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells one CTA covers
+   (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
+   mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and
+   y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp strip march, 28
+   columns per warp) or MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
+   memory; FP32-mixed only), or -1 for an unknown configuration. */
 enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,
        MHDB_KERNEL_MARCH_TMA = 3 };
 int mhdb_tile_config_count(int precision);
