@@ -227,13 +227,14 @@ struct PolicyMixed {
                                                       double dt, const Consts& k, double& smax,
                                                       const Op& op)
     {
-        const size_t o = static_cast<size_t>(gy) * g.pitch + gx;
-        float* __restrict__ oh = a.out.hi + o;
-        float* __restrict__ ol = a.out.lo + o;
+        // Plane bases are the same for every thread; the cell offset within a plane fits 32 bits
+        // (it is below the plane size), so each store address is one wide multiply-add.
+        const uint32_t o = static_cast<uint32_t>(gy) * static_cast<uint32_t>(g.pitch) +
+                           static_cast<uint32_t>(gx);
         const size_t pl = g.plane;
         update_ops<STAGE>(a, solid, L, dt, k, smax, op, [&](int c, float h, float l) {
-            oh[c * pl] = h;
-            ol[c * pl] = l;
+            (a.out.hi + static_cast<size_t>(c) * pl)[o] = h;
+            (a.out.lo + static_cast<size_t>(c) * pl)[o] = l;
         });
     }
     // The same with the results handed to st(c, hi, lo) instead of stored to the output planes.
