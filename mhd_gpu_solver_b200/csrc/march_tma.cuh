@@ -2,19 +2,23 @@
 // solid mask).
 //
 // The arithmetic is that of march_kernel.cuh (register-resident stencil, shuffle x sweep, every
-// slope limited once and every face evaluated once), so both kernels produce the same values.
-// What changes is how rows reach the warp: each warp runs a two-slot TMA pipeline per stream of
-// rows, driven by lane 0 and completed on mbarriers:
+// slope limited once and every face evaluated once; here the limiters return half slopes, the
+// same values): ideal solves give the register march's values bit for bit, non-ideal ones agree
+// to FP32 rounding (the compiler may contract the Ohm's-law products differently). What changes
+// is how rows reach the warp: each warp runs a two-slot TMA pipeline per stream of rows, driven
+// by lane 0 and completed on mbarriers:
 //   * halo stream: the stage input's 9 hi planes of row y + 2, columns x0 - 4 .. x0 + 31
 //     (box 36 x 1 x 9; the x origin x0 - 4 is a multiple of 4 floats, 16 bytes), issued two
 //     rows ahead of its use; lane l reads column x0 - 2 + l at offset l + 2;
 //   * own stream: the hi and lo planes of row y, owned columns x0 .. x0 + 27 (box 28 x 1 x 18),
 //     of the stage input and, in stage 2, of U^n (updated in place), issued two rows ahead.
-// Rows are addressed through the boundary map (periodic wrap / outflow clamp in y), so the
-// copies never leave the interior in y. Lanes whose column lies outside [0, nx) (x halo of the
-// first and last strips) load their values directly through the x map instead of from the box.
-// Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records kStatusWaitTimeout in
-// the Ctrl block, waits (bounded) for its copies still in flight and stops its strip.
+// Results leave through plain stores (ST = 0) or through TMA row stores from 1 or 2 staging
+// slots (ST = 1, 2). Rows are addressed through the boundary map (periodic wrap / outflow clamp in
+// y), so the copies never leave the interior in y. Lanes whose column lies outside [0, nx) (x
+// halo of the first and last strips) load their values directly through the x map instead of
+// from the box. Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records
+// kStatusWaitTimeout in the Ctrl block, waits (bounded) for its copies still in flight and stops
+// its strip.
 #pragma once
 
 #include "march_kernel.cuh"
