@@ -8,7 +8,8 @@
 //   * x neighbours come from warp shuffles: W(x+1), the left difference, the right neighbour's
 //     slope and the left face's flux;
 //   * every face is evaluated once per lane (x face x+1/2 and y face j+1/2), every slope is
-//     limited once, exactly as in the shared-memory tile kernel, so both produce the same values.
+//     limited once, with the same per-face and per-cell functions as the shared-memory tile
+//     kernel (both are held to the oracle at the same tolerances).
 // There is no shared memory and no barrier until the stage-2 signal-speed reduction. Boundary
 // conditions are the same index maps (periodic wrap / outflow clamp) applied to every load.
 // Non-ideal terms (NI): the current J of row y is carried like the primitives; J of row y + 1 is
