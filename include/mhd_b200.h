@@ -157,8 +157,9 @@ long long mhdb_launch_count(const mhdb_solver* h);
 
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the shared-memory tile
    kernel) serves every solve; the others serve solves without a mask (the strip-march ones ideal
-   and non-ideal solves, the other tile ones ideal solves only; a solve they do not serve runs
-   configuration 0) and are picked per grid size class by the autotuner
+   and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configuration 11 also
+   masked solves; a solve they do not serve runs configuration 0) and are picked per grid size
+   class by the autotuner
    (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells one CTA covers
    (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
    mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and
@@ -171,9 +172,9 @@ int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);
 int mhdb_tile_config_kind(int precision, int config);
-/* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves without a mask of at
-   least 1024 x 1024 cells run the TMA strip march (one warp per block), every other solve
-   configuration 0. */
+/* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves of at least 1024 x 1024
+   cells run the TMA strip march (one warp per block; configuration 11 for masked solves, the TMA
+   strip march that also serves masks), every other solve configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
 /* ---------------------------------------------------------------- batched form (additive)

@@ -68,10 +68,11 @@ template <class Policy, class Cfg, int L, bool NI, bool MASK>
 void fill_pair(StageKernels& k)
 {
     if constexpr (is_march_tma<Cfg>::value) {
-        static_assert(!MASK, "the strip-march kernel serves unmasked solves");
+        static_assert(!MASK || (Cfg::ST1 == 0 && Cfg::ST2 == 0),
+                      "masked TMA strip marches store through the lanes");
         static_assert(sizeof(typename Policy::T) == 4, "the TMA strip march is FP32-mixed only");
-        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI>;
-        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI>;
+        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;
+        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI, MASK>;
         k.tile_x = Cfg::NW * kMarchOwned;
         k.tile_y = Cfg::LY;
         k.threads = Cfg::NW * 32;
@@ -101,7 +102,8 @@ void fill_pair(StageKernels& k)
     }
 }
 
-// Every (limiter, non-ideal, mask) combination for the default configuration.
+// Every (limiter, non-ideal, mask) combination: the default configuration and the TMA strip
+// march that stores through the lanes.
 template <class Policy, class Cfg>
 StageKernels select_full(int lim, bool ni, bool mask)
 {

@@ -19,7 +19,7 @@ constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 int stage_config_count_f64() { return kCount; }
 
 // Without a chosen configuration the FP64 form runs the shared-memory tile kernel.
-int default_stage_config_f64(long long) { return 0; }
+int default_stage_config_f64(long long, bool) { return 0; }
 
 TileConfigInfo stage_config_info_f64(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }
 

@@ -30,10 +30,14 @@ constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 
 int stage_config_count_mixed() { return kCount; }
 
-// Without a chosen configuration: unmasked grids of at least 1024^2 cells run the TMA strip march
-// with one warp per block (configuration 9); smaller grids have too few 28-column strips to fill
-// the GPU with it and run the shared-memory tile kernel.
-int default_stage_config_mixed(long long cells) { return cells >= 1024LL * 1024 ? 9 : 0; }
+// Without a chosen configuration: grids of at least 1024^2 cells run the TMA strip march with one
+// warp per block (configuration 9; masked grids configuration 11, which stores through the lanes
+// and also serves masks); smaller grids have too few 28-column strips to fill the GPU with it and
+// run the shared-memory tile kernel.
+int default_stage_config_mixed(long long cells, bool mask)
+{
+    return cells >= 1024LL * 1024 ? (mask ? 11 : 9) : 0;
+}
 
 TileConfigInfo stage_config_info_mixed(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }
 
@@ -61,7 +65,7 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
     case 10:
         return select_unmasked<PolicyMixed, Cfg10>(limiter, nonideal, mask);
     case 11:
-        return select_unmasked<PolicyMixed, Cfg11>(limiter, nonideal, mask);
+        return select_full<PolicyMixed, Cfg11>(limiter, nonideal, mask);
     case 12:
         return select_unmasked<PolicyMixed, Cfg12>(limiter, nonideal, mask);
     default:

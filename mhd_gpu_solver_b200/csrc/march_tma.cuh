@@ -1,5 +1,5 @@
-// TMA-fed warp strip-march stage kernel of the FP32-mixed form (ideal or non-ideal GLM-MHD, no
-// solid mask).
+// TMA-fed warp strip-march stage kernel of the FP32-mixed form (ideal or non-ideal GLM-MHD, with
+// or without a solid mask).
 //
 // The arithmetic is that of march_kernel.cuh (register-resident stencil, shuffle x sweep, every
 // slope limited once and every face evaluated once; here the limiters return half slopes, the
@@ -16,7 +16,9 @@
 // slots (ST = 1, 2). Rows are addressed through the boundary map (periodic wrap / outflow clamp in
 // y), so the copies never leave the interior in y. Lanes whose column lies outside [0, nx) (x
 // halo of the first and last strips) load their values directly through the x map instead of
-// from the box. Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records
+// from the box. With a mask (MASK), solid cells are wall-filled when their row is converted to
+// primitives and their update takes the FP64 wall-fill path of PolicyMixed::update, through
+// plain stores. Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records
 // kStatusWaitTimeout in the Ctrl block, waits (bounded) for its copies still in flight and stops
 // its strip.
 #pragma once
@@ -51,7 +53,7 @@ constexpr size_t march_tma_smem_bytes(int warps)
     return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST>::kWarpBytes + 128;
 }
 
-template <int L, int STAGE, int LY, bool HF, int ST, bool NI>
+template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false>
 __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
                                                   int x0, int y0, int lane, unsigned char* wbase,
                                                   bool& failed_out)
@@ -127,8 +129,20 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     halo_issued = own_issued = nrows > 1 ? 2 : 1;
 
     auto load = [&](int y, Raw& r) { Policy::load_raw(a, g, sx, map_index(y, g.ny, g.bc_y), r); };
+    // Primitives of this lane's cell of row y. With a mask, an interior solid cell (by its own,
+    // unmapped coordinates: ghosts keep the stored values, include/mhd/time_integrator.hpp:46-49)
+    // is wall-filled in FP64 from its fluid neighbours, as in the tile kernel's load.
     auto prim = [&](int y, const Raw& r, T (&w)[9]) {
-        Policy::template raw_prim<STAGE, false>(a, g, sx, map_index(y, g.ny, g.bc_y), r, k, w);
+        const int sy = map_index(y, g.ny, g.bc_y);
+        if constexpr (MASK) {
+            if (a.walls && in_x && y >= 0 && y < g.ny && is_solid(a.mask, g, sx, sy)) {
+                double f[9];
+                Policy::template wall_fill<STAGE, true>(a, g, sx, sy, k.gm1, f);
+                Policy::prim_of(f, k, w);
+                return;
+            }
+        }
+        Policy::template raw_prim<STAGE, MASK>(a, g, sx, sy, r, k, w);
     };
 
     // Prologue (direct loads): rows y0-2 .. y0+1, slopes of rows y0-1 and y0, flux G(y0 - 1/2).
@@ -249,7 +263,18 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 __syncwarp();
             }
             const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
-            if (own) {
+            const bool solid = MASK && own && is_solid(a.mask, g, gx, y);
+            if (solid) {
+                // L = 0, and with walls the stored value is the wall fill (PolicyMixed::update
+                // reads its operands from global memory; plain stores only, ST == 0)
+                T Lc[9];
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    Lc[c] = -dF[c] * inv_dx - (Gp[c] - Gm[c]) * inv_dy;
+                }
+                Policy::template update<STAGE, true>(a, g, gx, y, true, Lc, Wm[8], psi_damp, dt, k,
+                                                     smax);
+            } else if (own) {
                 T Lc[9];
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
@@ -336,7 +361,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     return smax;
 }
 
-template <int L, int STAGE, int LY, int NW, int MINB, bool HF, int ST, bool NI>
+template <int L, int STAGE, int LY, int NW, int MINB, bool HF, int ST, bool NI, bool MASK = false>
 __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArgsMx a,
                                                                    const __grid_constant__ MarchTmaMaps m)
 {
@@ -352,7 +377,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArg
     double smax = 0.0;
     bool failed = false;
     if (x0 < a.geom.nx) { // warp-uniform
-        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(
+        static_assert(!MASK || ST == 0, "masked strips store through the lanes");
+        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI, MASK>(
             a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
             base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes, failed);
     }

@@ -343,17 +343,16 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     s.k = make_consts(h, p);
     const bool ni = s.k.ni_any != 0;
     StageKernels sk{};
-    // Tuned configurations serve unmasked solves (the tile ones other than 0 ideal solves only,
-    // the strip-march ones non-ideal solves too); every other solve uses configuration 0.
+    // Configurations other than 0 serve unmasked solves (the tile ones ideal solves only, the
+    // strip-march ones non-ideal solves too; FP32-mixed configuration 11 also masked solves);
+    // a solve the chosen configuration does not serve uses configuration 0.
     const long long cells = static_cast<long long>(h->grid.nx) * h->grid.ny;
-    int cfg = h->tile_config >= 0 ? h->tile_config
-                                  : (h->precision == MHDB_FP64 ? default_stage_config_f64(cells)
-                                                               : default_stage_config_mixed(cells));
-    if (h->has_mask) {
-        cfg = 0;
-    }
-    if (cfg != 0 && (h->precision == MHDB_FP64 ? select_stage_f64(p->limiter, ni, false, cfg)
-                                               : select_stage_mixed(p->limiter, ni, false, cfg))
+    int cfg = h->tile_config >= 0
+                  ? h->tile_config
+                  : (h->precision == MHDB_FP64 ? default_stage_config_f64(cells, h->has_mask)
+                                               : default_stage_config_mixed(cells, h->has_mask));
+    if (cfg != 0 && (h->precision == MHDB_FP64 ? select_stage_f64(p->limiter, ni, h->has_mask, cfg)
+                                               : select_stage_mixed(p->limiter, ni, h->has_mask, cfg))
                             .threads == 0) {
         cfg = 0;
     }

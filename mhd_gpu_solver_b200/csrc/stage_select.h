@@ -39,13 +39,14 @@ struct TileConfigInfo {
 int stage_config_count_f64();
 int stage_config_count_mixed();
 // Configuration used when none is chosen (mhdb_set_tile_config(h, -1), the default).
-int default_stage_config_f64(long long cells);
-int default_stage_config_mixed(long long cells);
+int default_stage_config_f64(long long cells, bool mask);
+int default_stage_config_mixed(long long cells, bool mask);
 TileConfigInfo stage_config_info_f64(int config);
 TileConfigInfo stage_config_info_mixed(int config);
 
-// Kernels of one configuration; config != 0 is available only for ideal, unmasked solves
-// (threads == 0 otherwise).
+// Kernels of one configuration; threads == 0 when the configuration does not serve the
+// combination (configurations other than 0 serve unmasked solves, and masked ones where they
+// store through the lanes).
 // Tensor maps of one TMA strip-march stage reading `in` and writing `out` (tma_maps.cu); false
 // with a message when the driver cannot encode them.
 bool encode_march_maps(const MixedState& in, const MixedState& out, const Geometry& g,

@@ -17,10 +17,11 @@ def to_c_params(p: orc.Params) -> _capi.Params:
 
 
 def gpu_solve(U0: np.ndarray, grid: orc.Grid, p: orc.Params, bc=(orc.PERIODIC, orc.PERIODIC),
-              mask=None, walls: bool = True, precision: int = _capi.FP64):
+              mask=None, walls: bool = True, precision: int = _capi.FP64, tile_config: int = -1):
     dev = _capi.DeviceSolver(grid.nx, grid.ny, grid.x_min, grid.x_max, grid.y_min, grid.y_max,
                              grid.ng, precision)
     try:
+        dev.set_tile_config(tile_config)
         dev.configure(bc[0], bc[1], mask, walls)
         dev.upload(np.ascontiguousarray(U0))
         cp = to_c_params(p)

@@ -415,3 +415,43 @@ def test_default_configuration_of_a_large_grid_matches_fp64():
         assert r32.steps == r64.steps == 6
         err = rel_l1(u32, u64)
         assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (kw, err)
+
+
+@pytest.mark.parametrize("bc", [(orc.OUTFLOW, orc.PERIODIC), (orc.PERIODIC, orc.OUTFLOW)])
+@pytest.mark.parametrize("walls", [True, False])
+@pytest.mark.parametrize("ni", [False, True])
+def test_masked_tma_strip_march_matches_oracle(bc, walls, ni):
+    """Masked solves on the strip-march configurations (FP32-mixed configuration 11 is the TMA
+    strip march that serves masks; the others fall back to the tile kernel): solids wall-filled
+    when their row is converted, solid updates through the FP64 wall-fill path, ghosts keeping
+    pre-fill values; against the FP64 oracle within the FP32-mixed tolerance."""
+    nx, ny = 61, 45
+    mask = _edge_mask(nx, ny, seed=11)
+    U0 = initial_state(wl.fourier_state(nx, ny, 6), 5.0 / 3.0, bc, mask, walls)
+    kw = NI_PARAMS if ni else {}
+    p = orc.Params(limiter=orc.VANLEER, max_steps=25, fixed_steps=True, **kw)
+    ref, tr, sr, _ = orc.solve(U0, orc.Grid(nx, ny), p, bc, mask, walls)
+    for cfg in _capi.tile_configs(_capi.FP32):
+        if not cfg["kind"].startswith("march"):
+            continue
+        got, tg, sg, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, mask, walls, precision=_capi.FP32,
+                              tile_config=cfg["config"])
+        assert sg == sr
+        assert abs(tg - tr) <= 1e-6 * max(1.0, tr)
+        err = rel_l1(got, ref)
+        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (cfg, err)
+
+
+def test_default_configuration_of_a_large_masked_grid_matches_fp64():
+    """A 1024^2 masked, non-ideal FP32-mixed solve without a chosen configuration runs the TMA
+    strip march that serves masks; it stays within the FP32-mixed tolerance of the FP64 form."""
+    n = 1024
+    bc = (orc.OUTFLOW, orc.PERIODIC)
+    mask = wl.circles_and_rectangles(n, n, 0)
+    U0 = initial_state(wl.fourier_state(n, n, 1), 5.0 / 3.0, bc, mask)
+    p = orc.Params(limiter=orc.VANLEER, max_steps=6, fixed_steps=True, **NI_PARAMS)
+    u64, _, s64, _ = _gpu(U0, orc.Grid(n, n), p, bc, mask)
+    u32, _, s32, _ = _gpu(U0, orc.Grid(n, n), p, bc, mask, precision=_capi.FP32)
+    assert s32 == s64 == 6
+    err = rel_l1(u32, u64)
+    assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), err
