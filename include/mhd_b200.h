@@ -158,8 +158,8 @@ long long mhdb_launch_count(const mhdb_solver* h);
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the shared-memory tile
    kernel) serves every solve; the others serve solves without a mask (the strip-march ones ideal
    and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configuration 11 also
-   masked solves; a solve they do not serve runs configuration 0) and are picked per grid size
-   class by the autotuner
+   masked solves; a solve they do not serve runs the default of its size, see below) and are
+   picked per grid size class by the autotuner
    (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells one CTA covers
    (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
    mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and

@@ -344,17 +344,21 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     const bool ni = s.k.ni_any != 0;
     StageKernels sk{};
     // Configurations other than 0 serve unmasked solves (the tile ones ideal solves only, the
-    // strip-march ones non-ideal solves too; FP32-mixed configuration 11 also masked solves);
-    // a solve the chosen configuration does not serve uses configuration 0.
+    // strip-march ones non-ideal solves too; FP32-mixed configuration 11 also masked solves). A
+    // solve the chosen configuration does not serve (e.g. a masked solve after an autotuner
+    // choice made on unmasked grids) uses the default configuration of its size, else 0.
     const long long cells = static_cast<long long>(h->grid.nx) * h->grid.ny;
-    int cfg = h->tile_config >= 0
-                  ? h->tile_config
-                  : (h->precision == MHDB_FP64 ? default_stage_config_f64(cells, h->has_mask)
-                                               : default_stage_config_mixed(cells, h->has_mask));
-    if (cfg != 0 && (h->precision == MHDB_FP64 ? select_stage_f64(p->limiter, ni, h->has_mask, cfg)
-                                               : select_stage_mixed(p->limiter, ni, h->has_mask, cfg))
-                            .threads == 0) {
-        cfg = 0;
+    const int dflt = h->precision == MHDB_FP64 ? default_stage_config_f64(cells, h->has_mask)
+                                               : default_stage_config_mixed(cells, h->has_mask);
+    auto serves = [&](int c) {
+        return c == 0 || (h->precision == MHDB_FP64
+                              ? select_stage_f64(p->limiter, ni, h->has_mask, c)
+                              : select_stage_mixed(p->limiter, ni, h->has_mask, c))
+                                 .threads != 0;
+    };
+    int cfg = h->tile_config >= 0 ? h->tile_config : dflt;
+    if (!serves(cfg)) {
+        cfg = serves(dflt) ? dflt : 0;
     }
     if (h->precision == MHDB_FP64) {
         sk = select_stage_f64(p->limiter, ni, h->has_mask, cfg);
