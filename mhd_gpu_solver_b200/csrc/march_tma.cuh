@@ -17,8 +17,8 @@
 // y), so the copies never leave the interior in y. Lanes whose column lies outside [0, nx) (x
 // halo of the first and last strips) load their values directly through the x map instead of
 // from the box. With a mask (MASK), solid cells are wall-filled when their row is converted to
-// primitives and their update takes the FP64 wall-fill path of PolicyMixed::update, through
-// plain stores. Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records
+// primitives, and a solid cell's update stores the conservative form of those filled
+// primitives (through plain stores). Each mbarrier wait is bounded (tma.cuh); on a timeout the warp records
 // kStatusWaitTimeout in the Ctrl block, waits (bounded) for its copies still in flight and stops
 // its strip.
 #pragma once
@@ -131,18 +131,65 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     auto load = [&](int y, Raw& r) { Policy::load_raw(a, g, sx, map_index(y, g.ny, g.bc_y), r); };
     // Primitives of this lane's cell of row y. With a mask, an interior solid cell (by its own,
     // unmapped coordinates: ghosts keep the stored values, include/mhd/time_integrator.hpp:46-49)
-    // is wall-filled in FP64 from its fluid neighbours, as in the tile kernel's load.
+    // is wall-filled from its first fluid interior neighbour in the order +x, -x, +y, -y, or set
+    // to the isolated state (include/mhd/mask.hpp:100-146). Filled values feed FP32 fluxes only,
+    // so the x neighbours' primitives come from the neighbour lanes (reflected: normal velocity
+    // negated, density and pressure floored at 1e-12), an isolated cell takes rho = p = 1 at rest
+    // with zero B and psi, and the remaining cases (a fluid y neighbour, or an x neighbour outside
+    // this warp) take the FP64 fill of the tile kernel from global memory.
     auto prim = [&](int y, const Raw& r, T (&w)[9]) {
         const int sy = map_index(y, g.ny, g.bc_y);
+        Policy::template raw_prim<STAGE, MASK>(a, g, sx, sy, r, k, w);
         if constexpr (MASK) {
-            if (a.walls && in_x && y >= 0 && y < g.ny && is_solid(a.mask, g, sx, sy)) {
+            if (!a.walls || y < 0 || y >= g.ny) { // warp-uniform
+                return;
+            }
+            const bool solid = in_x && is_solid(a.mask, g, sx, sy);
+            if (!__any_sync(kFull, solid)) {
+                return;
+            }
+            const bool fluid = in_x && !solid;
+            const bool fluid_e = __shfl_down_sync(kFull, fluid, 1) && lane < 31;
+            const bool fluid_w = __shfl_up_sync(kFull, fluid, 1) && lane > 0;
+            T we[9], ww[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                we[c] = __shfl_down_sync(kFull, w[c], 1);
+                ww[c] = __shfl_up_sync(kFull, w[c], 1);
+            }
+            if (!solid) {
+                return;
+            }
+            const T tiny = T(1e-12);
+            if (fluid_e || (fluid_w && lane > 0 && lane < 31 && !fluid_e)) {
+                // lane 31 never gets here (its +x neighbour is outside the warp); lane 0 only
+                // through fluid_e
+                const T* s = fluid_e ? we : ww;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    w[c] = s[c];
+                }
+                w[1] = -w[1];
+                w[0] = w[0] < tiny ? tiny : w[0];
+                w[4] = w[4] < tiny ? tiny : w[4];
+                return;
+            }
+            const bool edge = lane == 31 || (lane == 0 && !fluid_e);
+            const bool fluid_n = y + 1 < g.ny && !is_solid(a.mask, g, sx, y + 1);
+            const bool fluid_s = y > 0 && !is_solid(a.mask, g, sx, y - 1);
+            if (edge || fluid_n || fluid_s) {
                 double f[9];
                 Policy::template wall_fill<STAGE, true>(a, g, sx, sy, k.gm1, f);
                 Policy::prim_of(f, k, w);
                 return;
             }
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                w[c] = T(0);
+            }
+            w[0] = T(1);
+            w[4] = T(1);
         }
-        Policy::template raw_prim<STAGE, MASK>(a, g, sx, sy, r, k, w);
     };
 
     // Prologue (direct loads): rows y0-2 .. y0+1, slopes of rows y0-1 and y0, flux G(y0 - 1/2).
@@ -264,16 +311,35 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             }
             const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
             const bool solid = MASK && own && is_solid(a.mask, g, gx, y);
-            if (solid) {
-                // L = 0, and with walls the stored value is the wall fill (PolicyMixed::update
-                // reads its operands from global memory; plain stores only, ST == 0)
-                T Lc[9];
+            if (solid && a.walls) {
+                // L = 0 and the stored value is the wall fill of the stage input (tile kernel:
+                // PolicyMixed::update): stage 1 stores fill(U^n), stage 2 (U*_stored +
+                // fill(U*)) / 2. The fill is this row's filled primitives Wm, made conservative
+                // in FP64; plain stores only (ST == 0).
+                const double rho = Wm[0], vx = Wm[1], vy = Wm[2], vz = Wm[3];
+                const double bx = Wm[5], by = Wm[6], bz = Wm[7];
+                double f[9] = {rho, rho * vx, rho * vy, rho * vz,
+                               static_cast<double>(Wm[4]) * k.inv_gm1 +
+                                   0.5 * rho * (vx * vx + vy * vy + vz * vz) +
+                                   0.5 * (bx * bx + by * by + bz * bz),
+                               bx, by, bz, static_cast<double>(Wm[8])};
+                const size_t o = static_cast<size_t>(y) * g.pitch + gx;
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
-                    Lc[c] = -dF[c] * inv_dx - (Gp[c] - Gm[c]) * inv_dy;
+                    if constexpr (STAGE == 2) {
+                        f[c] = 0.5 * ((static_cast<double>(src[c * kTmaOwnW]) +
+                                       static_cast<double>(src[(9 + c) * kTmaOwnW])) + f[c]);
+                    }
+                    split_store(a.out, static_cast<size_t>(c) * g.plane + o, f[c]);
                 }
-                Policy::template update<STAGE, true>(a, g, gx, y, true, Lc, Wm[8], psi_damp, dt, k,
-                                                     smax);
+            } else if (solid) {
+                // without walls a solid cell only has L = 0
+                const T Lz[9] = {};
+                auto op = [&](int q) {
+                    return q < 18 ? src[q * kTmaOwnW]
+                                  : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
+                };
+                Policy::template update_ops<STAGE>(a, g, gx, y, true, Lz, dt, k, smax, op);
             } else if (own) {
                 T Lc[9];
 #pragma unroll
