@@ -150,6 +150,11 @@ def test_batch_errors():
         b.status(sid)
     with pytest.raises(ValueError, match="unknown solve id"):
         b.status(12345)
+    with pytest.raises(ValueError, match="unknown batch configuration"):
+        b.set_config(sid, -2)
+    with pytest.raises(ValueError, match="unknown batch configuration"):
+        b.set_config(sid, _capi.lib.mhdb_batch_config_count(_capi.FP32))
+    b.set_config(sid, -1)  # back to the choice by size
     b.close()
     assert math.isinf(fixed_params(3).t_end)
 
