@@ -165,7 +165,7 @@ long long mhdb_launch_count(const mhdb_solver* h);
    mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and
    y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp strip march, 28
    columns per warp) or MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
-   memory; FP32-mixed only), or -1 for an unknown configuration. */
+   memory), or -1 for an unknown configuration. */
 enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,
        MHDB_KERNEL_MARCH_TMA = 3 };
 int mhdb_tile_config_count(int precision);
@@ -174,7 +174,10 @@ int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, i
 int mhdb_tile_config_kind(int precision, int config);
 /* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves of at least 1024 x 1024
    cells run the TMA strip march (one warp per block; configuration 11 for masked solves, the TMA
-   strip march that also serves masks), every other solve configuration 0. */
+   strip march that also serves masks), smaller FP32-mixed ones configuration 0; FP64 solves
+   without a mask of at least 2048 x 2048 cells run the FP64 TMA strip march (configuration 7),
+   smaller ones the 320-thread tile kernel (configuration 2, non-ideal ones configuration 0),
+   masked FP64 solves configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
 /* ---------------------------------------------------------------- batched form (additive)

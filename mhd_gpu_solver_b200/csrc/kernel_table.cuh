@@ -70,14 +70,23 @@ void fill_pair(StageKernels& k)
     if constexpr (is_march_tma<Cfg>::value) {
         static_assert(!MASK || (Cfg::ST1 == 0 && Cfg::ST2 == 0),
                       "masked TMA strip marches store through the lanes");
-        static_assert(sizeof(typename Policy::T) == 4, "the TMA strip march is FP32-mixed only");
-        k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;
-        k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI, MASK>;
+        constexpr int E = static_cast<int>(sizeof(typename Policy::T));
+        if constexpr (E == 8) {
+            static_assert(!MASK && Cfg::ST1 == 0 && Cfg::ST2 == 0,
+                          "the FP64 TMA strip march serves unmasked solves, lane stores");
+            k.f64_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+                                          Policy>;
+            k.f64_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+                                          Policy>;
+        } else {
+            k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;
+            k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI, MASK>;
+        }
         k.tile_x = Cfg::NW * kMarchOwned;
         k.tile_y = Cfg::LY;
         k.threads = Cfg::NW * 32;
-        k.smem = march_tma_smem_bytes<1, Cfg::ST1>(Cfg::NW);
-        k.smem2 = march_tma_smem_bytes<2, Cfg::ST2>(Cfg::NW);
+        k.smem = march_tma_smem_bytes<1, Cfg::ST1, E>(Cfg::NW);
+        k.smem2 = march_tma_smem_bytes<2, Cfg::ST2, E>(Cfg::NW);
         return;
     } else if constexpr (is_march<Cfg>::value) {
         static_assert(!MASK, "the strip-march kernel serves unmasked solves");

@@ -31,13 +31,14 @@ namespace mhdb {
 
 // Shared memory of one warp: 2 halo slots, 2 own slots, ST staging slots for the row stores
 // (ST = 0: results are stored by the lanes; 1 or 2: TMA row stores through 1 or 2 staging slots),
-// then the 4 mbarriers.
-template <int STAGE, int ST>
+// then the 4 mbarriers. ELEM is the size of a stored value: 4 for the FP32-mixed state (a row
+// box holds 18 hi and lo planes), 8 for the FP64 state (9 planes).
+template <int STAGE, int ST, int ELEM = 4>
 struct MarchTmaLayout {
-    static constexpr int kHaloFloats = 9 * kTmaHaloW;             // 324 floats, 1296 B
-    static constexpr int kHaloBytes = kHaloFloats * 4;
-    static constexpr int kHaloSlot = (kHaloBytes + 127) / 128 * 128; // 1408 B
-    static constexpr int kOwnBoxBytes = 18 * kTmaOwnW * 4;          // 2016 B per box
+    static constexpr int kOwnPlanes = ELEM == 4 ? 18 : 9;
+    static constexpr int kHaloBytes = 9 * kTmaHaloW * ELEM;        // 1296 B (FP32), 2592 B (FP64)
+    static constexpr int kHaloSlot = (kHaloBytes + 127) / 128 * 128;
+    static constexpr int kOwnBoxBytes = kOwnPlanes * kTmaOwnW * ELEM; // 2016 B per box
     static constexpr int kOwnBoxSlot = (kOwnBoxBytes + 127) / 128 * 128; // 2048 B
     static constexpr int kOwnBoxes = STAGE == 1 ? 1 : 2;
     static constexpr int kOwnSlot = kOwnBoxes * kOwnBoxSlot;
@@ -47,21 +48,25 @@ struct MarchTmaLayout {
     static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
 };
 
-template <int STAGE, int ST>
+template <int STAGE, int ST, int ELEM = 4>
 constexpr size_t march_tma_smem_bytes(int warps)
 {
-    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST>::kWarpBytes + 128;
+    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST, ELEM>::kWarpBytes + 128;
 }
 
-template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false>
-__device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const MarchTmaMaps& m,
+template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false,
+          class Policy = PolicyMixed>
+__device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a,
+                                                  const MarchTmaMaps& m,
                                                   int x0, int y0, int lane, unsigned char* wbase,
                                                   bool& failed_out)
 {
-    using Policy = PolicyMixed;
-    using T = float;
-    using Raw = Policy::Raw;
-    using Lay = MarchTmaLayout<STAGE, ST>;
+    using T = typename Policy::T;
+    using Raw = typename Policy::Raw;
+    using Lay = MarchTmaLayout<STAGE, ST, sizeof(T)>;
+    static_assert(sizeof(T) == 4 || (ST == 0 && !MASK),
+                  "the FP64 TMA strip march stores through the lanes and serves unmasked solves");
+    constexpr int kOwnPlanes = Lay::kOwnPlanes;
     constexpr unsigned kFull = 0xffffffffu;
     const Geometry& g = a.geom;
     const Consts& k = a.k;
@@ -81,8 +86,8 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     const int y1 = min(y0 + LY, g.ny);
     const int nrows = y1 - y0;
 
-    const float* halo_f = reinterpret_cast<const float*>(wbase);
-    const float* own_f = reinterpret_cast<const float*>(wbase + 2 * Lay::kHaloSlot);
+    const T* halo_f = reinterpret_cast<const T*>(wbase);
+    const T* own_f = reinterpret_cast<const T*>(wbase + 2 * Lay::kHaloSlot);
     float* stg_f = reinterpret_cast<float*>(wbase + Lay::kStageOff);
     const uint32_t halo_s = smem_addr(wbase);
     const uint32_t own_s = halo_s + 2 * Lay::kHaloSlot;
@@ -263,7 +268,7 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             }
             halo_done = i + 1;
             if (in_x) {
-                const float* src = halo_f + slot * (Lay::kHaloSlot / 4) + lane + 2;
+                const T* src = halo_f + slot * (Lay::kHaloSlot / sizeof(T)) + lane + 2;
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
                     rn.v[c] = src[c * kTmaHaloW];
@@ -309,9 +314,17 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
                 }
                 __syncwarp();
             }
-            const float* src = own_f + slot * (Lay::kOwnSlot / 4) + (lane - 2);
+            const T* src = own_f + slot * (Lay::kOwnSlot / sizeof(T)) + (lane - 2);
+            // own-cell operand q: plane q of the stage input, then (stage 2) of U^n
+            auto op = [&](int q) {
+                return q < kOwnPlanes
+                           ? src[q * kTmaOwnW]
+                           : src[Lay::kOwnBoxSlot / sizeof(T) + (q - kOwnPlanes) * kTmaOwnW];
+            };
             const bool solid = MASK && own && is_solid(a.mask, g, gx, y);
-            if (solid && a.walls) {
+            if constexpr (!MASK) {
+                // no solid cells
+            } else if (solid && a.walls) {
                 // L = 0 and the stored value is the wall fill of the stage input (tile kernel:
                 // PolicyMixed::update): stage 1 stores fill(U^n), stage 2 (U*_stored +
                 // fill(U*)) / 2. The fill is this row's filled primitives Wm, made conservative
@@ -335,24 +348,17 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
             } else if (solid) {
                 // without walls a solid cell only has L = 0
                 const T Lz[9] = {};
-                auto op = [&](int q) {
-                    return q < 18 ? src[q * kTmaOwnW]
-                                  : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
-                };
                 Policy::template update_ops<STAGE>(a, g, gx, y, true, Lz, dt, k, smax, op);
-            } else if (own) {
+            }
+            if (own && !solid) {
                 T Lc[9];
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
                     Lc[c] = -dF[c] * inv_dx - (Gp[c] - Gm[c]) * inv_dy; // include/mhd/rhs.hpp:121
                 }
                 if (psi_damp != 0.0) {
-                    Lc[8] -= static_cast<float>(psi_damp) * Wm[8]; // include/mhd/rhs.hpp:219-225
+                    Lc[8] -= static_cast<T>(psi_damp) * Wm[8]; // include/mhd/rhs.hpp:219-225
                 }
-                auto op = [&](int q) {
-                    return q < 18 ? src[q * kTmaOwnW]
-                                  : src[Lay::kOwnBoxSlot / 4 + (q - 18) * kTmaOwnW];
-                };
                 if constexpr (ST > 0) {
                     float* dst = stg_f + (i % (ST > 0 ? ST : 1)) * (Lay::kOwnBoxSlot / 4) + (lane - 2);
                     Policy::template update_ops<STAGE>(a, false, Lc, dt, k, smax, op,
@@ -427,8 +433,9 @@ __device__ __forceinline__ double march_tma_strip(const StageArgsMx& a, const Ma
     return smax;
 }
 
-template <int L, int STAGE, int LY, int NW, int MINB, bool HF, int ST, bool NI, bool MASK = false>
-__global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArgsMx a,
+template <int L, int STAGE, int LY, int NW, int MINB, bool HF, int ST, bool NI, bool MASK = false,
+          class Policy = PolicyMixed>
+__global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const typename Policy::Args a,
                                                                    const __grid_constant__ MarchTmaMaps m)
 {
     if (a.ctrl->finished != 0) {
@@ -444,9 +451,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const StageArg
     bool failed = false;
     if (x0 < a.geom.nx) { // warp-uniform
         static_assert(!MASK || ST == 0, "masked strips store through the lanes");
-        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI, MASK>(
+        smax = march_tma_strip<L, STAGE, LY, HF, ST, NI, MASK, Policy>(
             a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
-            base + warp * MarchTmaLayout<STAGE, ST>::kWarpBytes, failed);
+            base + warp * MarchTmaLayout<STAGE, ST, sizeof(typename Policy::T)>::kWarpBytes,
+            failed);
     }
     if constexpr (STAGE == 2) {
         reduce_signal_speed_and_finish(smax, a.ctrl, a.k, gridDim.x * gridDim.y, true);

@@ -331,6 +331,7 @@ struct StepPlan {
     StageFnMx m1 = nullptr, m2 = nullptr;
     StageArgsMx b1{}, b2{};
     StageFnMxTma t1 = nullptr, t2 = nullptr; // TMA-fed FP32-mixed kernels (m1/m2 unused then)
+    StageFnF64Tma d1 = nullptr, d2 = nullptr; // TMA-fed FP64 kernels (s1/s2 unused then)
     MarchTmaMaps tm1{}, tm2{};
     dim3 grid, block;
     size_t smem = 0, smem2 = 0; // dynamic shared memory of stage 1 and stage 2
@@ -370,6 +371,15 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
                             h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
         s.a2 = StageArgsF64{us, static_cast<double*>(h->U), h->has_mask ? h->mask : nullptr,
                             h->ctrl, h->geom, s.k, h->walls ? 1 : 0};
+        if (sk.f64_tma1 != nullptr) {
+            s.d1 = sk.f64_tma1;
+            s.d2 = sk.f64_tma2;
+            std::string err;
+            if (!encode_march_maps_f64(u, us, h->geom, &s.tm1, &err) ||
+                !encode_march_maps_f64(us, u, h->geom, &s.tm2, &err)) {
+                throw ApiError{MHDB_CUDA_ERROR, err};
+            }
+        }
     } else {
         s.mixed = true;
         sk = select_stage_mixed(p->limiter, ni, h->has_mask, cfg);
@@ -399,7 +409,10 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     s.smem = sk.smem;
     s.smem2 = sk.smem2;
     const int b1 = static_cast<int>(s.smem), b2 = static_cast<int>(s.smem2);
-    if (!s.mixed) {
+    if (s.d1 != nullptr) {
+        MHDB_CHECK(cudaFuncSetAttribute(s.d1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+        MHDB_CHECK(cudaFuncSetAttribute(s.d2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
+    } else if (!s.mixed) {
         MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
         MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
     } else if (s.t1 != nullptr) {
@@ -414,7 +427,10 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
 
 void launch_stage(mhdb_solver* h, const StepPlan& s, int stage)
 {
-    if (!s.mixed) {
+    if (s.d1 != nullptr) {
+        (stage == 1 ? s.d1 : s.d2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
+            stage == 1 ? s.a1 : s.a2, stage == 1 ? s.tm1 : s.tm2);
+    } else if (!s.mixed) {
         (stage == 1 ? s.s1 : s.s2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
             stage == 1 ? s.a1 : s.a2);
     } else if (s.t1 != nullptr) {

@@ -18,11 +18,13 @@ namespace mhdb {
 using StageFnF64 = void (*)(StageArgsF64);
 using StageFnMx = void (*)(StageArgsMx);
 using StageFnMxTma = void (*)(StageArgsMx, MarchTmaMaps); // TMA-fed kernels take tensor maps
+using StageFnF64Tma = void (*)(StageArgsF64, MarchTmaMaps);
 
 struct StageKernels {
     StageFnF64 f64_stage1 = nullptr, f64_stage2 = nullptr;
     StageFnMx mx_stage1 = nullptr, mx_stage2 = nullptr;
     StageFnMxTma mx_tma1 = nullptr, mx_tma2 = nullptr;
+    StageFnF64Tma f64_tma1 = nullptr, f64_tma2 = nullptr;
     int tile_x = 0, tile_y = 0, threads = 0; // threads == 0: no such configuration
     size_t smem = 0, smem2 = 0;               // dynamic shared memory per block, stage 1 and 2
 };
@@ -51,6 +53,9 @@ TileConfigInfo stage_config_info_mixed(int config);
 // with a message when the driver cannot encode them.
 bool encode_march_maps(const MixedState& in, const MixedState& out, const Geometry& g,
                        MarchTmaMaps* maps, std::string* err);
+// The same for the FP64 state (9 double planes).
+bool encode_march_maps_f64(const double* in, const double* out, const Geometry& g,
+                           MarchTmaMaps* maps, std::string* err);
 
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);

@@ -13,11 +13,12 @@
 
 namespace mhdb {
 
-// Tensor maps of one strip-march stage (stage_mixed.cuh state): 3D views (x, y, plane) of the
-// stage input and output buffers over the 18 float planes (9 hi, then 9 lo) of a mixed state.
+// Tensor maps of one strip-march stage: 3D views (x, y, plane) of the stage input and output
+// buffers. For a mixed state (stage_mixed.cuh) they span its 18 float planes (9 hi, then 9 lo):
 //   in_halo: stage input, box {kTmaHaloW, 1, 9}    (hi planes of one row, x halo included)
 //   in_own:  stage input, box {kTmaOwnW, 1, 18}    (hi and lo of a warp's owned columns)
 //   out_own: stage output, box {kTmaOwnW, 1, 18}   (stage 2 only: U^n, updated in place)
+// For an FP64 state they span its 9 double planes and every box holds all 9.
 struct MarchTmaMaps {
     CUtensorMap in_halo;
     CUtensorMap in_own;
