@@ -180,6 +180,46 @@ int mhdb_tile_config_kind(int precision, int config);
    masked FP64 solves configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
+/* ---------------------------------------------------------------- strips of one grid (additive)
+
+   One grid split into y strips, one solver per strip (on one GPU or on several): each strip's
+   solver holds its owned rows plus overlap rows copied from its neighbours (outflow y rule at the
+   strip's ends, which only corrupts overlap rows), so every step runs the same kernels as a whole
+   grid. The reference has no multi-GPU form; the step rule stays that of
+   include/mhd/time_integrator.hpp:62-106 with one global dt:
+
+     mhdb_set_cell_size(h, dx, dy)    the whole grid's cell size (a strip's extent / rows may
+                                      round differently; default: the grid's extent / cells)
+     mhdb_set_reduce_rows(h, y0, y1)  rows [y0, y1) of this solver's interior are its owned rows:
+                                      only they enter the CFL reduction and the diagnostics
+     mhdb_strip_begin(h, p, n)        start a deferred solve (n >= 0: n steps; n < 0: to p->t_end)
+                                      and reduce the owned rows' signal speed into ch_bits
+     (host: ch_bits = max over all strips, written back to each strip)
+     mhdb_strip_finish(h)             dt, c_h and the clock from the combined maximum
+     mhdb_strip_step(h)               one RK2 step (both stages), its reduction left in ch_bits
+     (host: combine, then mhdb_strip_finish, then copy overlap rows between neighbours)
+     mhdb_strip_poll / mhdb_strip_end the clock, finished flag and result, as mhdb_solve
+
+   All strips take the same dt, so they finish at the same step. Calls out of this order return
+   MHDB_INVALID_ARGUMENT; mhdb_solve / mhdb_solve_steps end a deferred solve. */
+typedef struct mhdb_strip_state {
+    void* state;      /* device: U^n, planes of `plane` elements, rows of `pitch` elements */
+    void* ch_bits;    /* device: 8-byte running signal-speed max (IEEE bits of a double >= 0) */
+    long long pitch;  /* elements per row (>= nx) */
+    long long plane;  /* elements per plane (pitch * ny) */
+    int planes;       /* 9 (FP64) or 18 (FP32-mixed: 9 hi planes, then 9 lo planes) */
+    int elem_bytes;   /* 8 (FP64) or 4 (FP32-mixed) */
+} mhdb_strip_state;
+
+int mhdb_set_cell_size(mhdb_solver* h, double dx, double dy);
+int mhdb_set_reduce_rows(mhdb_solver* h, int y0, int y1);
+int mhdb_strip_view(mhdb_solver* h, mhdb_strip_state* out);
+int mhdb_strip_begin(mhdb_solver* h, const mhdb_params* params, int nsteps);
+int mhdb_strip_step(mhdb_solver* h);
+int mhdb_strip_finish(mhdb_solver* h);
+int mhdb_strip_poll(mhdb_solver* h, int* finished, int* steps, double* t);
+int mhdb_strip_end(mhdb_solver* h, mhdb_result* result);
+
 /* ---------------------------------------------------------------- batched form (additive)
 
    A batch advances many independent solves of uneven sizes together: every RK2 step is one

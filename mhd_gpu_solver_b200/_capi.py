@@ -31,7 +31,8 @@ EXPORTS = (
     "mhdb_batch_remove", "mhdb_batch_step", "mhdb_batch_status", "mhdb_batch_download",
     "mhdb_batch_info", "mhdb_batch_stream", "mhdb_generate", "mhdb_batch_add_generated",
     "mhdb_batch_launch", "mhdb_batch_poll", "mhdb_batch_config_count", "mhdb_batch_config_info",
-    "mhdb_batch_set_config",
+    "mhdb_batch_set_config", "mhdb_set_cell_size", "mhdb_set_reduce_rows", "mhdb_strip_view", "mhdb_strip_begin",
+    "mhdb_strip_step", "mhdb_strip_finish", "mhdb_strip_poll", "mhdb_strip_end",
 )
 
 
@@ -63,6 +64,11 @@ class Diag(C.Structure):
     _fields_ = [("mass", C.c_double), ("energy", C.c_double), ("div_b_max", C.c_double),
                 ("div_b_l2", C.c_double), ("rho_min", C.c_double), ("p_min", C.c_double),
                 ("finite", C.c_int)]
+
+
+class StripState(C.Structure):
+    _fields_ = [("state", C.c_void_p), ("ch_bits", C.c_void_p), ("pitch", C.c_longlong),
+                ("plane", C.c_longlong), ("planes", C.c_int), ("elem_bytes", C.c_int)]
 
 
 class Init(C.Structure):
@@ -134,6 +140,14 @@ def _load() -> C.CDLL:
         "mhdb_batch_add_generated": ([b, C.POINTER(Grid), C.POINTER(Params), C.c_int, C.c_int,
                                       C.POINTER(Init), C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mhdb_generate": ([h, C.POINTER(Init), C.POINTER(Params)], C.c_int),
+        "mhdb_set_cell_size": ([h, C.c_double, C.c_double], C.c_int),
+        "mhdb_set_reduce_rows": ([h, C.c_int, C.c_int], C.c_int),
+        "mhdb_strip_view": ([h, C.POINTER(StripState)], C.c_int),
+        "mhdb_strip_begin": ([h, C.POINTER(Params), C.c_int], C.c_int),
+        "mhdb_strip_step": ([h], C.c_int),
+        "mhdb_strip_finish": ([h], C.c_int),
+        "mhdb_strip_poll": ([h, C.POINTER(C.c_int), C.POINTER(C.c_int), _PD], C.c_int),
+        "mhdb_strip_end": ([h, C.POINTER(Result)], C.c_int),
     })
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -281,6 +295,37 @@ class DeviceSolver:
 
     def set_tile_config(self, config: int) -> None:
         raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
+
+    # Deferred solves of one strip of a split grid (strips.py drives them).
+    def set_cell_size(self, dx: float, dy: float) -> None:
+        raise_for(lib.mhdb_set_cell_size(self._h, float(dx), float(dy)), self._h)
+
+    def set_reduce_rows(self, y0: int, y1: int) -> None:
+        raise_for(lib.mhdb_set_reduce_rows(self._h, int(y0), int(y1)), self._h)
+
+    def strip_view(self) -> StripState:
+        v = StripState()
+        raise_for(lib.mhdb_strip_view(self._h, C.byref(v)), self._h)
+        return v
+
+    def strip_begin(self, params: Params, nsteps: int) -> None:
+        raise_for(lib.mhdb_strip_begin(self._h, C.byref(params), int(nsteps)), self._h)
+
+    def strip_step(self) -> None:
+        raise_for(lib.mhdb_strip_step(self._h), self._h)
+
+    def strip_finish(self) -> None:
+        raise_for(lib.mhdb_strip_finish(self._h), self._h)
+
+    def strip_poll(self) -> tuple[bool, int, float]:
+        f, n, t = C.c_int(), C.c_int(), C.c_double()
+        raise_for(lib.mhdb_strip_poll(self._h, C.byref(f), C.byref(n), C.byref(t)), self._h)
+        return bool(f.value), n.value, t.value
+
+    def strip_end(self) -> Result:
+        r = Result()
+        raise_for(lib.mhdb_strip_end(self._h, C.byref(r)), self._h)
+        return r
 
 
 KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma"}

@@ -687,6 +687,8 @@ void add_solve(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, 
     s.geom.bc_x = bc_x;
     s.geom.bc_y = bc_y;
     s.geom.plane = static_cast<size_t>(s.geom.pitch) * grid->ny;
+    s.geom.ry0 = 0;
+    s.geom.ry1 = grid->ny;
     const size_t bytes = 9 * s.geom.plane * 8;
     check(cudaMallocFromPoolAsync(&s.U, bytes, b->pool, b->stream), "cudaMallocFromPoolAsync(U)");
     const cudaError_t e2 = cudaMallocFromPoolAsync(&s.Us, bytes, b->pool, b->stream);

@@ -64,10 +64,10 @@ __global__ void __launch_bounds__(kDiagThreads) diag_partial(Loader ld, const ui
                                                             double* partial)
 {
     double acc[kDiagFields] = {0.0, 0.0, 0.0, 0.0, INFINITY, INFINITY, 0.0};
-    const long long n = static_cast<long long>(g.nx) * g.ny;
+    const long long n = static_cast<long long>(g.nx) * (g.ry1 - g.ry0);
     for (long long c = blockIdx.x * static_cast<long long>(kDiagThreads) + threadIdx.x; c < n;
          c += static_cast<long long>(gridDim.x) * kDiagThreads) {
-        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        const int x = static_cast<int>(c % g.nx), y = g.ry0 + static_cast<int>(c / g.nx);
         double u[9];
         ld.cell(g, mask, fill, gm1, x, y, u);
         const double rho = u[0], E = u[4];

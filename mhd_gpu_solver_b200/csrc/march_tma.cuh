@@ -361,7 +361,7 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                 }
                 if constexpr (ST > 0) {
                     float* dst = stg_f + (i % (ST > 0 ? ST : 1)) * (Lay::kOwnBoxSlot / 4) + (lane - 2);
-                    Policy::template update_ops<STAGE>(a, false, Lc, dt, k, smax, op,
+                    Policy::template update_ops<STAGE>(a, !reduce_row(g, y), Lc, dt, k, smax, op,
                                                        [&](int c, float h, float l) {
                                                            dst[c * kTmaOwnW] = h;
                                                            dst[(9 + c) * kTmaOwnW] = l;

@@ -143,6 +143,8 @@ int mhdb_solve_steps_noalloc_f64(const mhdb_grid* grid, int bc_x, int bc_y,
     g.bc_x = bc_x;
     g.bc_y = bc_y;
     g.plane = cells;
+    g.ry0 = 0;
+    g.ry1 = grid->ny;
 
     // Per-solve constants, as make_consts in solver.cu.
     Consts k{};

@@ -18,7 +18,16 @@ struct Geometry {
     int pitch;
     int bc_x, bc_y;
     size_t plane;
+    // Rows [ry0, ry1) of the interior whose cells enter the signal-speed reduction and the
+    // diagnostics: 0 and ny for a whole grid; the owned rows of one strip of a grid split into
+    // strips with overlap rows (the overlap rows are copies of a neighbour's rows).
+    int ry0, ry1;
 };
+
+__device__ __forceinline__ bool reduce_row(const Geometry& g, int y)
+{
+    return y >= g.ry0 && y < g.ry1;
+}
 
 // Per-solve constants, all computed on the host in FP64 exactly as the reference computes them.
 struct Consts {
@@ -46,7 +55,10 @@ struct Ctrl {
     int max_steps;
     int finished;
     int status;
-    int pad;
+    // Nonzero: the reduction's last CTA leaves the running max in ch_bits and does not run
+    // finish_step; the host combines ch_bits over the strips of a split grid (max) and then
+    // launches finish_step_kernel.
+    int defer;
 };
 
 // Boundary rule as an index map onto the interior (include/boundary_conditions/
@@ -129,7 +141,11 @@ __device__ __forceinline__ void reduce_signal_speed_and_finish(double v, Ctrl* c
     __syncthreads();
     if (is_last != 0 && threadIdx.x == 0) {
         __threadfence();
-        finish_step(ctrl, k, advance);
+        if (ctrl->defer == 0) {
+            finish_step(ctrl, k, advance);
+        } else {
+            ctrl->arrived = 0u;
+        }
     }
 }
 

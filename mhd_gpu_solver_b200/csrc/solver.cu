@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -196,6 +197,8 @@ struct Prof {
     int kind;
 };
 
+struct StepPlan;
+
 } // namespace
 
 struct mhdb_solver {
@@ -207,6 +210,7 @@ struct mhdb_solver {
     cudaStream_t stream = nullptr;
 
     Geometry geom{};
+    double dx = 0.0, dy = 0.0; // cell size: the grid's extent / cells unless set explicitly
     int nxt = 0, nyt = 0;
     size_t ntot = 0;
 
@@ -239,6 +243,14 @@ struct mhdb_solver {
     double prof_ms[2] = {0.0, 0.0};
     int prof_n[2] = {0, 0};
     long long launches = 0;
+
+    // A deferred solve (mhdb_strip_*): its plan, whether it runs a fixed number of steps, its
+    // t_end, and which call comes next (a finish after begin / step, a step after finish).
+    std::unique_ptr<StepPlan> strip;
+    bool strip_fixed = false;
+    double strip_t_end = 0.0;
+    bool strip_advance = false;
+    bool strip_due = false;
 };
 
 namespace {
@@ -277,8 +289,8 @@ struct DeviceGuard {
 Consts make_consts(const mhdb_solver* h, const mhdb_params* p)
 {
     Consts k{};
-    const double dx = (h->grid.x_max - h->grid.x_min) / static_cast<double>(h->grid.nx);
-    const double dy = (h->grid.y_max - h->grid.y_min) / static_cast<double>(h->grid.ny);
+    const double dx = h->dx;
+    const double dy = h->dy;
     k.gamma = p->gamma;
     k.gm1 = p->gamma - 1.0;
     k.inv_gm1 = 1.0 / (p->gamma - 1.0);
@@ -483,7 +495,8 @@ std::vector<double> plan_key(const mhdb_solver* h, const mhdb_params* p, const S
             static_cast<double>(p->ambipolar), p->eta_ohm, p->eta_hall, p->eta_ambipolar,
             static_cast<double>(h->grid.nx), static_cast<double>(h->grid.ny),
             static_cast<double>(h->tile_config),
-            h->grid.x_min, h->grid.x_max, h->grid.y_min, h->grid.y_max};
+            h->grid.x_min, h->grid.x_max, h->grid.y_min, h->grid.y_max, h->dx, h->dy,
+            static_cast<double>(h->geom.ry0), static_cast<double>(h->geom.ry1)};
 }
 
 void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n)
@@ -531,7 +544,7 @@ void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n
     MHDB_CHECK(cudaGetLastError());
 }
 
-void start_solve(mhdb_solver* h, const StepPlan& s, double t_end, int max_steps)
+void start_solve(mhdb_solver* h, const StepPlan& s, double t_end, int max_steps, int defer = 0)
 {
     Ctrl c{};
     c.t = 0.0;
@@ -544,6 +557,7 @@ void start_solve(mhdb_solver* h, const StepPlan& s, double t_end, int max_steps)
     c.max_steps = max_steps;
     c.finished = 0;
     c.status = 0;
+    c.defer = defer;
     *h->ctrl_host = c;
     MHDB_CHECK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice,
                                h->stream));
@@ -620,6 +634,54 @@ void release(mhdb_solver* h)
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
+// Before a solve: the state left by an earlier solve is wall-filled, as the reference leaves it.
+void prepare_solve(mhdb_solver* h, const mhdb_params* p)
+{
+    if (h->solved_since_upload && h->has_mask && h->walls) {
+        // The state is the result of an earlier solve, which the reference leaves wall-filled
+        // (time_integrator.hpp:101-104); apply that fill now so that ghosts of solid edge
+        // cells see the filled values, as after a download/upload round trip.
+        const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+        if (h->precision == MHDB_FP64) {
+            fill_solids_f64<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                static_cast<double*>(h->U), h->mask, h->geom, h->last_gm1);
+        } else {
+            fill_solids_mixed<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
+                mixed_view(h->U, h->geom), h->mask, h->geom, h->last_gm1);
+        }
+        ++h->launches;
+        MHDB_CHECK(cudaGetLastError());
+    }
+    h->last_gm1 = p->gamma - 1.0;
+    h->solved_since_upload = true;
+}
+
+// After a solve: the Ctrl block read back by read_ctrl into the result, or the solve's error.
+void collect_result(mhdb_solver* h, bool time_based, double t_end, mhdb_result* r)
+{
+    const Ctrl& c = *h->ctrl_host;
+    if ((c.status & kStatusWaitTimeout) != 0) {
+        throw ApiError{MHDB_CUDA_ERROR, "stage kernel: a bulk-copy wait exceeded its limit"};
+    }
+    if ((c.status & kStatusBadDt) != 0) {
+        throw ApiError{MHDB_BAD_TIMESTEP, "ssp_rk2_step requires positive dt"};
+    }
+    r->t = c.t;
+    r->steps = c.steps;
+    r->c_h = c.c_h;
+    if (time_based && c.t < t_end) {
+        throw ApiError{MHDB_MAX_STEPS, "solve: reached max_steps before t_end"};
+    }
+}
+
+// finish_step of a deferred solve, after the host has combined ch_bits over the strips.
+__global__ void finish_step_kernel(Ctrl* ctrl, Consts k, int advance)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ctrl->finished == 0) {
+        finish_step(ctrl, k, advance != 0);
+    }
+}
+
 int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result* r)
 {
     return guarded(h, [&] {
@@ -628,23 +690,9 @@ int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result
             throw ApiError{MHDB_INVALID_ARGUMENT, "result must not be NULL"};
         }
         const StepPlan s = make_plan(h, p);
-        if (h->solved_since_upload && h->has_mask && h->walls) {
-            // The state is the result of an earlier solve, which the reference leaves wall-filled
-            // (time_integrator.hpp:101-104); apply that fill now so that ghosts of solid edge
-            // cells see the filled values, as after a download/upload round trip.
-            const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
-            if (h->precision == MHDB_FP64) {
-                fill_solids_f64<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
-                    static_cast<double*>(h->U), h->mask, h->geom, h->last_gm1);
-            } else {
-                fill_solids_mixed<<<launch_blocks(n, 256), 256, 0, h->stream>>>(
-                    mixed_view(h->U, h->geom), h->mask, h->geom, h->last_gm1);
-            }
-            ++h->launches;
-            MHDB_CHECK(cudaGetLastError());
-        }
-        h->last_gm1 = p->gamma - 1.0;
-        h->solved_since_upload = true;
+        h->strip.reset(); // a solve ends any deferred solve of this handle
+        h->strip_due = false;
+        prepare_solve(h, p);
         if (fixed_steps >= 0) {
             start_solve(h, s, static_cast<double>(INFINITY), fixed_steps);
             launch_steps(h, p, s, fixed_steps);
@@ -675,19 +723,7 @@ int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result
                 batch = std::clamp(est, 1, 256);
             }
         }
-        const Ctrl& c = *h->ctrl_host;
-        if ((c.status & kStatusWaitTimeout) != 0) {
-            throw ApiError{MHDB_CUDA_ERROR, "stage kernel: a bulk-copy wait exceeded its limit"};
-        }
-        if ((c.status & kStatusBadDt) != 0) {
-            throw ApiError{MHDB_BAD_TIMESTEP, "ssp_rk2_step requires positive dt"};
-        }
-        r->t = c.t;
-        r->steps = c.steps;
-        r->c_h = c.c_h;
-        if (fixed_steps < 0 && c.t < p->t_end) {
-            throw ApiError{MHDB_MAX_STEPS, "solve: reached max_steps before t_end"};
-        }
+        collect_result(h, fixed_steps < 0, p->t_end, r);
     });
 }
 
@@ -746,6 +782,10 @@ int mhdb_create(const mhdb_grid* grid, int precision, mhdb_solver** out)
         h->geom.bc_x = kPeriodic;
         h->geom.bc_y = kPeriodic;
         h->geom.plane = static_cast<size_t>(h->geom.pitch) * grid->ny;
+        h->geom.ry0 = 0;
+        h->geom.ry1 = grid->ny;
+        h->dx = (grid->x_max - grid->x_min) / static_cast<double>(grid->nx);
+        h->dy = (grid->y_max - grid->y_min) / static_cast<double>(grid->ny);
         const size_t bytes = 9 * h->geom.plane * 8; // FP64 or two FP32 halves
         MHDB_CHECK(cudaMalloc(&h->U, bytes));
         MHDB_CHECK(cudaMalloc(&h->Us, bytes));
@@ -964,9 +1004,9 @@ int mhdb_diagnostics(mhdb_solver* h, const mhdb_params* params, mhdb_diag* out)
                                       sizeof(double) * kDiagFields));
         }
         const Consts k = make_consts(h, params);
-        const double dx = (h->grid.x_max - h->grid.x_min) / static_cast<double>(h->grid.nx);
-        const double dy = (h->grid.y_max - h->grid.y_min) / static_cast<double>(h->grid.ny);
-        const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+        const double dx = h->dx;
+        const double dy = h->dy;
+        const long long n = static_cast<long long>(h->grid.nx) * (h->geom.ry1 - h->geom.ry0);
         const int blocks = static_cast<int>(std::min<long long>(kDiagBlocks, (n + kDiagThreads - 1) / kDiagThreads));
         const int fill = (h->has_mask && h->walls) ? 1 : 0;
         if (h->precision == MHDB_FP64) {
@@ -1075,6 +1115,122 @@ int mhdb_set_tile_config(mhdb_solver* h, int config)
     }
     h->tile_config = config;
     return MHDB_OK;
+}
+
+int mhdb_set_reduce_rows(mhdb_solver* h, int y0, int y1)
+{
+    return guarded(h, [&] {
+        if (y0 < 0 || y1 > h->grid.ny || y0 >= y1) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "reduce rows must satisfy 0 <= y0 < y1 <= ny"};
+        }
+        if (h->strip) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "a deferred solve is running"};
+        }
+        h->geom.ry0 = y0;
+        h->geom.ry1 = y1;
+    });
+}
+
+int mhdb_set_cell_size(mhdb_solver* h, double dx, double dy)
+{
+    return guarded(h, [&] {
+        if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy)) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "cell size must be positive and finite"};
+        }
+        if (h->strip) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "a deferred solve is running"};
+        }
+        h->dx = dx;
+        h->dy = dy;
+    });
+}
+
+int mhdb_strip_view(mhdb_solver* h, mhdb_strip_state* out)
+{
+    return guarded(h, [&] {
+        if (out == nullptr) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "out must not be NULL"};
+        }
+        out->state = h->U;
+        out->ch_bits = &h->ctrl->ch_bits;
+        out->pitch = h->geom.pitch;
+        out->plane = static_cast<long long>(h->geom.plane);
+        out->planes = h->precision == MHDB_FP64 ? 9 : 18;
+        out->elem_bytes = h->precision == MHDB_FP64 ? 8 : 4;
+    });
+}
+
+int mhdb_strip_begin(mhdb_solver* h, const mhdb_params* params, int nsteps)
+{
+    return guarded(h, [&] {
+        validate_params(params, nsteps < 0);
+        h->strip.reset();
+        auto plan = std::make_unique<StepPlan>(make_plan(h, params));
+        prepare_solve(h, params);
+        h->strip_fixed = nsteps >= 0;
+        h->strip_t_end = params->t_end;
+        start_solve(h, *plan, nsteps >= 0 ? static_cast<double>(INFINITY) : params->t_end,
+                    nsteps >= 0 ? nsteps : params->max_steps, 1);
+        h->strip = std::move(plan);
+        h->strip_advance = false;
+        h->strip_due = true;
+    });
+}
+
+int mhdb_strip_step(mhdb_solver* h)
+{
+    return guarded(h, [&] {
+        if (!h->strip || h->strip_due) {
+            throw ApiError{MHDB_INVALID_ARGUMENT,
+                           "strip step: no deferred solve, or its reduction awaits mhdb_strip_finish"};
+        }
+        launch_step_direct(h, *h->strip);
+        MHDB_CHECK(cudaGetLastError());
+        h->strip_advance = true;
+        h->strip_due = true;
+    });
+}
+
+int mhdb_strip_finish(mhdb_solver* h)
+{
+    return guarded(h, [&] {
+        if (!h->strip || !h->strip_due) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "strip finish: no reduction awaits it"};
+        }
+        finish_step_kernel<<<1, 1, 0, h->stream>>>(h->ctrl, h->strip->k, h->strip_advance ? 1 : 0);
+        ++h->launches;
+        MHDB_CHECK(cudaGetLastError());
+        h->strip_due = false;
+    });
+}
+
+int mhdb_strip_poll(mhdb_solver* h, int* finished, int* steps, double* t)
+{
+    return guarded(h, [&] {
+        if (!h->strip) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "strip poll: no deferred solve"};
+        }
+        read_ctrl(h);
+        if (finished != nullptr) *finished = h->ctrl_host->finished;
+        if (steps != nullptr) *steps = h->ctrl_host->steps;
+        if (t != nullptr) *t = h->ctrl_host->t;
+    });
+}
+
+int mhdb_strip_end(mhdb_solver* h, mhdb_result* result)
+{
+    return guarded(h, [&] {
+        if (!h->strip || h->strip_due) {
+            throw ApiError{MHDB_INVALID_ARGUMENT,
+                           "strip end: no deferred solve, or its reduction awaits mhdb_strip_finish"};
+        }
+        if (result == nullptr) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "result must not be NULL"};
+        }
+        h->strip.reset();
+        read_ctrl(h);
+        collect_result(h, !h->strip_fixed, h->strip_t_end, result);
+    });
 }
 
 } // extern "C"

@@ -172,7 +172,7 @@ struct PolicyF64 {
                 r2[c] = 0.5 * (un[c] + uin[c]) + half_dt * L[c];
                 out[c * pl] = r2[c];
             }
-            if (!solid) {
+            if (!solid && reduce_row(g, gy)) {
                 smax = vmax(smax, signal_speed(r2, k));
             }
         }
@@ -187,10 +187,10 @@ __global__ void __launch_bounds__(NT) cfl_init_kernel_f64(const double* __restri
                                                          int has_mask)
 {
     double smax = 0.0;
-    const long long ncell = static_cast<long long>(g.nx) * g.ny;
+    const long long ncell = static_cast<long long>(g.nx) * (g.ry1 - g.ry0);
     for (long long c = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; c < ncell;
          c += static_cast<long long>(gridDim.x) * NT) {
-        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        const int x = static_cast<int>(c % g.nx), y = g.ry0 + static_cast<int>(c / g.nx);
         if (has_mask && is_solid(mask, g, x, y)) {
             continue;
         }

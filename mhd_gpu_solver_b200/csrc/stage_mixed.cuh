@@ -232,14 +232,17 @@ struct PolicyMixed {
         const uint32_t o = static_cast<uint32_t>(gy) * static_cast<uint32_t>(g.pitch) +
                            static_cast<uint32_t>(gx);
         const size_t pl = g.plane;
-        update_ops<STAGE>(a, solid, L, dt, k, smax, op, [&](int c, float h, float l) {
+        update_ops<STAGE>(a, solid || !reduce_row(g, gy), L, dt, k, smax, op,
+                          [&](int c, float h, float l) {
             (a.out.hi + static_cast<size_t>(c) * pl)[o] = h;
             (a.out.lo + static_cast<size_t>(c) * pl)[o] = l;
         });
     }
-    // The same with the results handed to st(c, hi, lo) instead of stored to the output planes.
+    // The same with the results handed to st(c, hi, lo) instead of stored to the output planes;
+    // no_speed (a solid cell, or a row outside the reduction rows) keeps the cell out of the
+    // signal-speed max.
     template <int STAGE, class Op, class St>
-    static __device__ __forceinline__ void update_ops(const Args& a, bool solid,
+    static __device__ __forceinline__ void update_ops(const Args& a, bool no_speed,
                                                       const float (&L)[9], double dt,
                                                       const Consts& k, double& smax, const Op& op,
                                                       const St& st)
@@ -284,7 +287,7 @@ struct PolicyMixed {
                 st(c, h, l);
                 rf[c] = h;
             }
-            if (!solid) {
+            if (!no_speed) {
                 smax = vmax(smax, static_cast<double>(signal_speed_f(rf, k)));
             }
         }
@@ -298,10 +301,10 @@ __global__ void __launch_bounds__(NT) cfl_init_kernel_mixed(const MixedState u,
                                                            int has_mask)
 {
     double smax = 0.0;
-    const long long ncell = static_cast<long long>(g.nx) * g.ny;
+    const long long ncell = static_cast<long long>(g.nx) * (g.ry1 - g.ry0);
     for (long long c = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; c < ncell;
          c += static_cast<long long>(gridDim.x) * NT) {
-        const int x = static_cast<int>(c % g.nx), y = static_cast<int>(c / g.nx);
+        const int x = static_cast<int>(c % g.nx), y = g.ry0 + static_cast<int>(c / g.nx);
         if (has_mask && is_solid(mask, g, x, y)) {
             continue;
         }
