@@ -18,9 +18,13 @@ zone-updates/s (interior cells x steps / device seconds).
   own headers into oracle/_ref, on all host cores, on a bounded number of steps of the same
   4096^2 state (MC limiter: the reference has no van Leer).
 
+* ``batched``, ``masked_nonideal``, ``served``: the batched, masked non-ideal and served
+  workloads (rank 0). ``strips``: the 4096^2 grid split into 2 y strips on this GPU (strips.py)
+  against the same grid as one solver.
+
 ``--impl reference`` times that reference CPU solver alone as the reference arm.
-Multi-GPU: the operator does not shard (replicas only); each rank runs the same workload on its
-own GPU and the value is the sum over ranks divided by the slowest rank's time.
+Multi-GPU: the measured operator runs replicas; each rank runs the same workload on its own GPU
+and the value is the sum over ranks divided by the slowest rank's time.
 """
 
 from __future__ import annotations
@@ -67,6 +71,8 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--masked-steps", type=int, default=300,
                     help="RK2 steps of the masked non-ideal 2048^2 leg (0 skips it)")
+    ap.add_argument("--strip-steps", type=int, default=100,
+                    help="RK2 steps of the 2-strip split of the 4096^2 grid (0 skips it)")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests of the served stream (0 skips it)")
     ap.add_argument("--serve-side", default="128,1024")
@@ -329,11 +335,70 @@ def bench_batched(nsolves: int, steps: int, seed: int = 1) -> dict:
             "gpu_launches": launches}
 
 
+def bench_strips(U: np.ndarray, n: int, steps: int, count: int = 2) -> dict:
+    """The n^2 periodic Fourier grid split into `count` y strips on this GPU (strips.py: one
+    solver and stream per strip, 6 overlap rows, combined CFL maximum and overlap-row copies on
+    the device, stepped by the host), FP32-mixed, against the same grid as one solver. Device
+    time on the host stream that waits for every strip; the strips' host loop is inside it."""
+    import torch
+
+    from mhd_gpu_solver_b200 import _capi
+    from mhd_gpu_solver_b200.strips import OVERLAP, StripSolver
+
+    params = _capi.make_params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=_capi.VANLEER)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with StripSolver(n, n, _capi.FP32, strips=count, distributed=False) as ss:
+        ss.upload(U)
+        ss.solve_steps(params, 3)  # warm-up: kernel attributes, stream waits
+        ss.upload(U)
+        main = torch.cuda.current_stream()
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record(main)
+        r = ss.solve_steps(params, steps)
+        for e in ss.engines:
+            main.wait_stream(e.stream)
+        e1.record(main)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        split = ss.gather()
+    dev = _capi.DeviceSolver(n, n, precision=_capi.FP32)
+    try:
+        dev.configure(_capi.BC_PERIODIC, _capi.BC_PERIODIC)
+        dev.upload(U)
+        dev.solve_steps(params, 3)
+        dev.upload(U)
+        stream = torch.cuda.ExternalStream(dev.stream())
+        w0, w1 = ev(), ev()
+        torch.cuda.synchronize()
+        w0.record(stream)
+        dev.solve_steps(params, steps)
+        w1.record(stream)
+        torch.cuda.synchronize()
+        ms_whole = w0.elapsed_time(w1)
+        whole = dev.download()[:, 2:-2, 2:-2]
+    finally:
+        dev.close()
+    num = np.abs(split - whole).reshape(9, -1).sum(axis=1)
+    den = np.abs(whole).reshape(9, -1).sum(axis=1)
+    l1 = num / np.where(den > 0, den, 1.0)
+    cells = float(n) * n * steps
+    return {"workload": f"{n}^2 periodic Fourier, FP32-mixed, van Leer, {count} y strips of "
+                        f"{n // count} rows + {OVERLAP} overlap rows per side on one GPU, "
+                        f"{steps} steps",
+            "zone_updates_per_s": cells / (ms * 1e-3), "ms": ms, "steps": r[1],
+            "whole_grid_zone_updates_per_s": cells / (ms_whole * 1e-3),
+            "ratio_to_whole_grid": ms_whole / ms,
+            "exchange_bytes_per_step": 2 * count * OVERLAP * n * 18 * 4,
+            "l1_vs_whole_grid_max": float(np.max(l1[[0, 1, 2, 4, 5, 6]]))}
+
+
 def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
     """The non-ideal, masked workload: n^2, the seeded Fourier state (generated on the device),
     Ohmic 1e-3, Hall 1e-2, ambipolar 1e-3, 12 circles and 6 rectangles of reflective walls,
     outflow in x and periodic in y, van Leer, `steps` RK2 steps, FP64 plain vs FP32-mixed (both
-    on the shared-memory tile kernel, the masked path). Reports each form's zone-updates/s, the
+    on their masked default kernels: FP64 the shared-memory tile kernel, FP32-mixed the masked
+    TMA strip march). Reports each form's zone-updates/s, the
     FP32-mixed L1 error against the FP64 result, and the FP64 div-B norms and mass/energy
     drift."""
     import torch
@@ -565,6 +630,8 @@ def main():
         line["batched"] = bench_batched(args.batch_solves, args.batch_steps)
     if rank == 0 and args.masked_steps > 0:
         line["masked_nonideal"] = bench_masked_nonideal(2048, args.masked_steps)
+    if rank == 0 and args.strip_steps > 0:
+        line["strips"] = bench_strips(U, n, args.strip_steps)
     if rank == 0 and args.serve_requests > 0:
         side = tuple(int(v) for v in args.serve_side.split(","))
         tend = tuple(float(v) for v in args.serve_tend.split(","))

@@ -101,10 +101,11 @@ class _Comm:
     """Who holds which strip, and the collectives between the processes that hold them. Every
     process holds a contiguous block of ``count / world`` strips."""
 
-    def __init__(self, count: int, group=None):
+    def __init__(self, count: int, group=None, distributed: bool | None = None):
         import torch.distributed as dist
 
-        self.dist = dist if dist.is_available() and dist.is_initialized() else None
+        up = dist.is_available() and dist.is_initialized()
+        self.dist = dist if (up if distributed is None else distributed) else None
         self.group = group
         self.rank = self.dist.get_rank(group) if self.dist else 0
         self.world = self.dist.get_world_size(group) if self.dist else 1
@@ -247,12 +248,14 @@ class StripSolver:
 
     ``engine`` builds the solver of one strip (default: ``DeviceStrip`` on the current CUDA
     device); it gets (strip, nx, ny, precision, domain, ng, bc_x, bc_y, mask_rows, walls).
+    ``distributed``: None spreads the strips over the processes of ``group`` when
+    torch.distributed is initialized; False keeps every strip in this process.
     """
 
     def __init__(self, nx: int, ny: int, precision: int, *, strips: int | None = None,
                  domain=(0.0, 1.0, 0.0, 1.0), ng: int = 2, bc=(0, 0), mask=None,
                  walls: bool = True, group=None, engine=None, overlap: int = OVERLAP,
-                 tile_config: int = -1):
+                 tile_config: int = -1, distributed: bool | None = None):
         from . import _capi
 
         if bc[0] == _capi.BC_REFLECTIVE or bc[1] == _capi.BC_REFLECTIVE:
@@ -262,7 +265,9 @@ class StripSolver:
         self.domain = tuple(float(v) for v in domain)
         self.bc = (int(bc[0]), int(bc[1]))
         self.periodic_y = self.bc[1] == _capi.BC_PERIODIC
-        self.comm = _Comm(strips if strips is not None else _world(group), group)
+        if strips is None and distributed is False:
+            raise ValueError("in-process strips need an explicit strip count")
+        self.comm = _Comm(strips if strips is not None else _world(group), group, distributed)
         count = self.comm.per * self.comm.world
         self.plan = plan_strips(ny, count, self.periodic_y, overlap)
         self.mask = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)

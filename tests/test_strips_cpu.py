@@ -224,6 +224,15 @@ def _rank(rank, world, port, case, per_rank, q):
                             timeout=datetime.timedelta(seconds=60))
     try:
         got, res = _split_solve(case, per_rank * world)
+        # the same split kept inside this process while the process group is up
+        grid, p, U0, mask, c = _problem(case)
+        with strips.StripSolver(grid.nx, grid.ny, 0, strips=2, bc=c["bc"], mask=mask,
+                                domain=(grid.x_min, grid.x_max, grid.y_min, grid.y_max),
+                                engine=OracleStrip, distributed=False) as ss:
+            ss.upload(U0)
+            local_res = (ss.solve_steps(p, c["steps"]) if c["steps"] >= 0 else ss.solve(p))
+            local = ss.gather()
+        assert local_res == res and np.array_equal(local, got)
         q.put((rank, got, res))
     finally:
         dist.barrier()
