@@ -157,8 +157,8 @@ long long mhdb_launch_count(const mhdb_solver* h);
 
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the shared-memory tile
    kernel) serves every solve; the others serve solves without a mask (the strip-march ones ideal
-   and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configuration 11 also
-   masked solves; a solve they do not serve runs the default of its size, see below) and are
+   and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configuration 11 and
+   FP64 configuration 7 also masked solves; a solve they do not serve runs the default of its size, see below) and are
    picked per grid size class by the autotuner
    (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells one CTA covers
    (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
@@ -174,10 +174,10 @@ int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, i
 int mhdb_tile_config_kind(int precision, int config);
 /* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves of at least 1024 x 1024
    cells run the TMA strip march (one warp per block; configuration 11 for masked solves, the TMA
-   strip march that also serves masks), smaller FP32-mixed ones configuration 0; FP64 solves
-   without a mask of at least 2048 x 2048 cells run the FP64 TMA strip march (configuration 7),
-   smaller ones the 320-thread tile kernel (configuration 2, non-ideal ones configuration 0),
-   masked FP64 solves configuration 0. */
+   strip march that also serves masks), smaller FP32-mixed ones configuration 0; FP64 solves of
+   at least 2048 x 2048 cells run the FP64 TMA strip march (configuration 7, which also serves
+   masks), smaller ones the 320-thread tile kernel (configuration 2, non-ideal ones configuration
+   0), smaller masked FP64 solves configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
 /* ---------------------------------------------------------------- strips of one grid (additive)

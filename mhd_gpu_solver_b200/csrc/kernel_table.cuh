@@ -43,8 +43,7 @@ struct MarchCfg {
     static constexpr bool MARCH = true;
 };
 
-// TMA-fed strip-march configuration (FP32-mixed form only): NW warps per block, LY rows per
-// warp, MINB blocks per SM.
+// TMA-fed strip-march configuration: NW warps per block, LY rows per warp, MINB blocks per SM.
 template <int NW_, int LY_, int MINB_, bool HF_ = true, int ST1_ = 1, int ST2_ = 0>
 struct MarchTmaCfg {
     static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
@@ -72,11 +71,11 @@ void fill_pair(StageKernels& k)
                       "masked TMA strip marches store through the lanes");
         constexpr int E = static_cast<int>(sizeof(typename Policy::T));
         if constexpr (E == 8) {
-            static_assert(!MASK && Cfg::ST1 == 0 && Cfg::ST2 == 0,
-                          "the FP64 TMA strip march serves unmasked solves, lane stores");
-            k.f64_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+            static_assert(Cfg::ST1 == 0 && Cfg::ST2 == 0,
+                          "the FP64 TMA strip march stores through the lanes");
+            k.f64_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                           Policy>;
-            k.f64_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+            k.f64_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                           Policy>;
         } else {
             k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;

@@ -21,15 +21,16 @@ constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 
 int stage_config_count_f64() { return kCount; }
 
-// Without a chosen configuration: unmasked FP64 grids of at least 2048^2 cells run the TMA strip
-// march (configuration 7: 10 one-warp blocks per SM), smaller ones the 320-thread tile kernel
-// (configuration 2; non-ideal solves then run configuration 0), masked grids configuration 0.
+// Without a chosen configuration: FP64 grids of at least 2048^2 cells run the TMA strip march
+// (configuration 7: 10 one-warp blocks per SM, masked grids included); smaller ones the 320-thread
+// tile kernel (configuration 2; non-ideal solves then run configuration 0), smaller masked grids
+// configuration 0.
 int default_stage_config_f64(long long cells, bool mask)
 {
-    if (mask) {
-        return 0;
+    if (cells >= 2048LL * 2048) {
+        return 7;
     }
-    return cells >= 2048LL * 2048 ? 7 : 2;
+    return mask ? 0 : 2;
 }
 
 TileConfigInfo stage_config_info_f64(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }
@@ -50,7 +51,7 @@ StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config)
     case 6:
         return select_unmasked<PolicyF64, Cfg6>(limiter, nonideal, mask);
     case 7:
-        return select_unmasked<PolicyF64, Cfg7>(limiter, nonideal, mask);
+        return select_full<PolicyF64, Cfg7>(limiter, nonideal, mask);
     default:
         return select_full<PolicyF64, Cfg0>(limiter, nonideal, mask);
     }

@@ -64,8 +64,7 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
     using T = typename Policy::T;
     using Raw = typename Policy::Raw;
     using Lay = MarchTmaLayout<STAGE, ST, sizeof(T)>;
-    static_assert(sizeof(T) == 4 || (ST == 0 && !MASK),
-                  "the FP64 TMA strip march stores through the lanes and serves unmasked solves");
+    static_assert(sizeof(T) == 4 || ST == 0, "the FP64 TMA strip march stores through the lanes");
     constexpr int kOwnPlanes = Lay::kOwnPlanes;
     constexpr unsigned kFull = 0xffffffffu;
     const Geometry& g = a.geom;
@@ -150,6 +149,16 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                 return;
             }
             const bool solid = in_x && is_solid(a.mask, g, sx, sy);
+            if constexpr (sizeof(T) == 8) {
+                // FP64: every solid cell takes the FP64 fill of the tile kernel (its operations
+                // and order, so the filled values are those of the oracle)
+                if (solid) {
+                    double f[9];
+                    Policy::template wall_fill<STAGE, true>(a, g, sx, sy, k.gm1, f);
+                    Policy::prim_of(f, k, w);
+                }
+                return;
+            }
             if (!__any_sync(kFull, solid)) {
                 return;
             }
@@ -324,6 +333,14 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             const bool solid = MASK && own && is_solid(a.mask, g, gx, y);
             if constexpr (!MASK) {
                 // no solid cells
+            } else if constexpr (sizeof(T) == 8) {
+                if (solid) {
+                    // FP64: the tile kernel's solid update, from global memory: L = 0; with walls
+                    // stage 1 stores fill(U^n) and stage 2 (U*_stored + fill(U*)) / 2
+                    T Lz[9] = {};
+                    Policy::template update<STAGE, true>(a, g, gx, y, true, Lz, T(0), 0.0, dt,
+                                                         k, smax);
+                }
             } else if (solid && a.walls) {
                 // L = 0 and the stored value is the wall fill of the stage input (tile kernel:
                 // PolicyMixed::update): stage 1 stores fill(U^n), stage 2 (U*_stored +

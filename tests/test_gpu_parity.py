@@ -442,6 +442,33 @@ def test_masked_tma_strip_march_matches_oracle(bc, walls, ni):
         assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (cfg, err)
 
 
+@pytest.mark.parametrize("bc", [(orc.OUTFLOW, orc.PERIODIC), (orc.PERIODIC, orc.OUTFLOW)])
+@pytest.mark.parametrize("walls", [True, False])
+@pytest.mark.parametrize("ni", [False, True])
+def test_masked_fp64_tma_strip_march_matches_oracle(bc, walls, ni):
+    """Masked FP64 solves on the FP64 strip-march configurations (configuration 7 is the TMA
+    strip march that serves masks: solid cells take the tile kernel's FP64 fill and solid update
+    from global memory): every component within the FP64 bar of the oracle, same step count."""
+    nx, ny = 61, 45
+    mask = _edge_mask(nx, ny, seed=11)
+    U0 = initial_state(wl.fourier_state(nx, ny, 6), 5.0 / 3.0, bc, mask, walls)
+    kw = NI_PARAMS if ni else {}
+    p = orc.Params(limiter=orc.VANLEER, max_steps=25, fixed_steps=True, **kw)
+    ref, tr, sr, cr = orc.solve(U0, orc.Grid(nx, ny), p, bc, mask, walls)
+    served = 0
+    for cfg in _capi.tile_configs(_capi.FP64):
+        if cfg["kind"] != "march_tma":
+            continue
+        got, tg, sg, cg = _gpu(U0, orc.Grid(nx, ny), p, bc, mask, walls,
+                               tile_config=cfg["config"])
+        assert sg == sr
+        assert abs(tg - tr) <= 1e-12 * max(1.0, tr) and abs(cg - cr) <= 1e-12 * cr
+        err = rel_l1(got, ref)
+        assert np.all(err <= FP64_L1), (cfg, err)
+        served += 1
+    assert served >= 1
+
+
 def test_default_configuration_of_a_large_masked_grid_matches_fp64():
     """A 1024^2 masked, non-ideal FP32-mixed solve without a chosen configuration runs the TMA
     strip march that serves masks; it stays within the FP32-mixed tolerance of the FP64 form."""
