@@ -9,6 +9,11 @@
   -fno-trapping-math``; cmake/MHDCompilerFlags.cmake:29-35) for two ISA levels
   (x86-64-v4 = AVX-512F, x86-64-v3 = AVX2+FMA). Built only where the reference checkout
   exists; the built files travel with the repository to machines that lack it.
+* ``oracle/_ref/cuda_bench_reference`` and ``oracle/_ref/cuda_bench_b200``: the timing driver
+  ``cuda_backend_bench.cpp`` over the reference's DeviceSolver interface, linked with the
+  reference's own CUDA backend (``src/cuda/cuda_solver.cu`` compiled by nvcc for sm_100a with the
+  reference's flags: C++20, -O3; CMakeLists.txt:87-101) and with the B200 adapter: a same-box
+  baseline of the reference's GPU path.
 """
 
 from __future__ import annotations
@@ -129,7 +134,37 @@ def build_ref_with_b200(force: bool = False) -> list[str]:
     return outs
 
 
+def build_cuda_bench(force: bool = False) -> list[str]:
+    """The DeviceSolver timing driver against both CUDA backends (no-op without the reference
+    checkout, nvcc or the B200 library)."""
+    lib = os.path.join(PKG_DIR, "libmhd_b200.so")
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    if not reference_available() or not os.path.exists(lib) or not os.path.exists(nvcc):
+        return []
+    os.makedirs(REF_DIR, exist_ok=True)
+    inc = os.path.join(REFERENCE_ROOT, "include")
+    drv = os.path.join(HERE, "cuda_backend_bench.cpp")
+    host = ["g++", "-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-fno-trapping-math",
+            "-ffp-contract=fast", "-march=x86-64-v3", "-pthread", "-DMHD_HAS_CUDA=1", "-I", inc]
+    outs = []
+    src_cu = os.path.join(REFERENCE_ROOT, "src", "cuda", "cuda_solver.cu")
+    obj = os.path.join(REF_DIR, "reference_cuda_solver.o")
+    ref_bin = os.path.join(REF_DIR, "cuda_bench_reference")
+    if force or _stale(ref_bin, [src_cu, drv]):
+        _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++20", "-O3",
+              "-DMHD_HAS_CUDA=1", "-I", inc, "-c", src_cu, "-o", obj])
+        _run(host + [drv, obj, "-L/usr/local/cuda/lib64", "-lcudart", "-o", ref_bin])
+    outs.append(ref_bin)
+    b200_bin = os.path.join(REF_DIR, "cuda_bench_b200")
+    if force or _stale(b200_bin, [drv, ADAPTER, lib]):
+        _run(host + ["-I", REPO_INCLUDE, drv, ADAPTER, "-o", b200_bin, "-L", PKG_DIR,
+                     "-l:libmhd_b200.so", "-Wl,-rpath,$ORIGIN/../../mhd_gpu_solver_b200"])
+    outs.append(b200_bin)
+    return outs
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
     print(build_ref_with_b200(force="--force" in sys.argv))
+    print(build_cuda_bench(force="--force" in sys.argv))
