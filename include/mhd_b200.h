@@ -164,10 +164,12 @@ long long mhdb_launch_count(const mhdb_solver* h);
    (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
    mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and
    y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp strip march, 28
-   columns per warp) or MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
-   memory), or -1 for an unknown configuration. */
+   columns per warp), MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
+   memory) or MHDB_KERNEL_MARCH_TMA_DELTA (the same for the FP32-mixed increment form: stage 1
+   stores the FP32 increment dt L instead of U*, stage 2 reads U^n + increment; unmasked solves),
+   or -1 for an unknown configuration. */
 enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,
-       MHDB_KERNEL_MARCH_TMA = 3 };
+       MHDB_KERNEL_MARCH_TMA = 3, MHDB_KERNEL_MARCH_TMA_DELTA = 4 };
 int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);
@@ -203,7 +205,9 @@ int mhdb_set_tile_config(mhdb_solver* h, int config);
    All strips take the same dt, so they finish at the same step. Calls out of this order return
    MHDB_INVALID_ARGUMENT; mhdb_solve / mhdb_solve_steps end a deferred solve. */
 typedef struct mhdb_strip_state {
-    void* state;      /* device: U^n, planes of `plane` elements, rows of `pitch` elements */
+    void* state;      /* device: U^n, planes of `plane` elements, rows of `pitch` elements; the
+                         FP32-mixed increment form alternates between two buffers, so query it
+                         again after mhdb_strip_step */
     void* ch_bits;    /* device: 8-byte running signal-speed max (IEEE bits of a double >= 0) */
     long long pitch;  /* elements per row (>= nx) */
     long long plane;  /* elements per plane (pitch * ny) */

@@ -328,7 +328,7 @@ class DeviceSolver:
         return r
 
 
-KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma"}
+KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma", 4: "march_tma_delta"}
 
 
 def tile_configs(precision: int) -> list[dict]:

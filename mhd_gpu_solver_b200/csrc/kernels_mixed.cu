@@ -17,6 +17,8 @@ using Cfg9 = MarchTmaCfg<1, 32, 16>;
 using Cfg10 = MarchTmaCfg<4, 32, 4, true, 0>;
 using Cfg11 = MarchTmaCfg<1, 32, 16, true, 0>;
 using Cfg12 = MarchTmaCfg<1, 64, 16>;
+using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, true>; // increment form
+using Cfg14 = MarchTmaCfg<1, 64, 16, true, 0, 0, true>; // increment form, 64-row segments
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
@@ -24,7 +26,8 @@ constexpr TileConfigInfo kInfo[] = {
     {112, 64, 128, 3, kKindMarch},     {112, 32, 128, 4, kKindMarchTma},
     {56, 32, 64, 8, kKindMarchTma},    {28, 32, 32, 16, kKindMarchTma},
     {112, 32, 128, 4, kKindMarchTma},  {28, 32, 32, 16, kKindMarchTma},
-    {28, 64, 32, 16, kKindMarchTma}};
+    {28, 64, 32, 16, kKindMarchTma},   {28, 32, 32, 16, kKindMarchTmaDelta},
+    {28, 64, 32, 16, kKindMarchTmaDelta}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -68,6 +71,10 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_full<PolicyMixed, Cfg11>(limiter, nonideal, mask);
     case 12:
         return select_unmasked<PolicyMixed, Cfg12>(limiter, nonideal, mask);
+    case 13:
+        return select_unmasked<PolicyMixed, Cfg13>(limiter, nonideal, mask);
+    case 14:
+        return select_unmasked<PolicyMixed, Cfg14>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

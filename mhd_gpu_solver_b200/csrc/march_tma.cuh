@@ -32,26 +32,38 @@ namespace mhdb {
 // Shared memory of one warp: 2 halo slots, 2 own slots, ST staging slots for the row stores
 // (ST = 0: results are stored by the lanes; 1 or 2: TMA row stores through 1 or 2 staging slots),
 // then the 4 mbarriers. ELEM is the size of a stored value: 4 for the FP32-mixed state (a row
-// box holds 18 hi and lo planes), 8 for the FP64 state (9 planes).
-template <int STAGE, int ST, int ELEM = 4>
+// box holds 18 hi and lo planes), 8 for the FP64 state (9 planes). KIND 1 is the increment form
+// (stage_delta.cuh): stage 1 has no own stream (its update needs no own-cell operand); stage 2
+// has two halo boxes (hi(U^n), then delta) and own boxes delta (9 planes), then U^n (18).
+template <int STAGE, int ST, int ELEM = 4, int KIND = 0>
 struct MarchTmaLayout {
+    static constexpr bool kDelta = KIND == 1;
     static constexpr int kOwnPlanes = ELEM == 4 ? 18 : 9;
-    static constexpr int kHaloBytes = 9 * kTmaHaloW * ELEM;        // 1296 B (FP32), 2592 B (FP64)
-    static constexpr int kHaloSlot = (kHaloBytes + 127) / 128 * 128;
+    static constexpr int kHaloBoxBytes = 9 * kTmaHaloW * ELEM;   // 1296 B (FP32), 2592 B (FP64)
+    static constexpr int kHaloBoxSlot = (kHaloBoxBytes + 127) / 128 * 128;
+    static constexpr int kHaloBoxes = (kDelta && STAGE == 2) ? 2 : 1;
+    static constexpr int kHaloBytes = kHaloBoxes * kHaloBoxBytes; // transaction bytes per row
+    static constexpr int kHaloSlot = kHaloBoxes * kHaloBoxSlot;
     static constexpr int kOwnBoxBytes = kOwnPlanes * kTmaOwnW * ELEM; // 2016 B per box
     static constexpr int kOwnBoxSlot = (kOwnBoxBytes + 127) / 128 * 128; // 2048 B
-    static constexpr int kOwnBoxes = STAGE == 1 ? 1 : 2;
-    static constexpr int kOwnSlot = kOwnBoxes * kOwnBoxSlot;
-    static constexpr int kOwnTx = kOwnBoxes * kOwnBoxBytes;       // transaction bytes per row
+    // own box A (the stage input's own cells; delta in the increment form) and box B (U^n)
+    static constexpr int kOwnPlanesA = kDelta ? 9 : kOwnPlanes;
+    static constexpr int kOwnABytes = kOwnPlanesA * kTmaOwnW * ELEM;
+    static constexpr int kOwnBOff = (kOwnABytes + 127) / 128 * 128; // byte offset of box B
+    static constexpr int kOwnBoxes = kDelta ? (STAGE == 1 ? 0 : 2) : (STAGE == 1 ? 1 : 2);
+    static constexpr int kOwnSlot = kOwnBoxes == 0 ? 0 : (kOwnBoxes == 1 ? kOwnBoxSlot
+                                                                        : kOwnBOff + kOwnBoxSlot);
+    static constexpr int kOwnTx = kOwnBoxes == 0 ? 0 : (kOwnBoxes == 1 ? kOwnBoxBytes
+                                                                      : kOwnABytes + kOwnBoxBytes);
     static constexpr int kStageOff = 2 * kHaloSlot + 2 * kOwnSlot;
     static constexpr int kBarOff = kStageOff + ST * kOwnBoxSlot;
     static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
 };
 
-template <int STAGE, int ST, int ELEM = 4>
+template <int STAGE, int ST, int ELEM = 4, int KIND = 0>
 constexpr size_t march_tma_smem_bytes(int warps)
 {
-    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST, ELEM>::kWarpBytes + 128;
+    return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST, ELEM, KIND>::kWarpBytes + 128;
 }
 
 template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false,
@@ -63,9 +75,10 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
 {
     using T = typename Policy::T;
     using Raw = typename Policy::Raw;
-    using Lay = MarchTmaLayout<STAGE, ST, sizeof(T)>;
+    using Lay = MarchTmaLayout<STAGE, ST, sizeof(T), Policy::kLayout>;
     static_assert(sizeof(T) == 4 || ST == 0, "the FP64 TMA strip march stores through the lanes");
-    constexpr int kOwnPlanes = Lay::kOwnPlanes;
+    static_assert(!Lay::kDelta || (ST == 0 && !MASK),
+                  "the increment form serves unmasked solves and stores through the lanes");
     constexpr unsigned kFull = 0xffffffffu;
     const Geometry& g = a.geom;
     const Consts& k = a.k;
@@ -107,18 +120,24 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
     auto issue_halo = [&](int i) {
         const uint32_t slot = static_cast<uint32_t>(i & 1);
         const uint32_t bar = bar_s + 8 * slot;
+        const int yy = map_index(y0 + 2 + i, g.ny, g.bc_y);
         mbar_arrive_expect_tx(bar, Lay::kHaloBytes);
-        tma_load_3d(halo_s + slot * Lay::kHaloSlot, &m.in_halo, bar, x0 - 4,
-                    map_index(y0 + 2 + i, g.ny, g.bc_y), 0);
+        tma_load_3d(halo_s + slot * Lay::kHaloSlot, &m.in_halo, bar, x0 - 4, yy, 0);
+        if constexpr (Lay::kHaloBoxes == 2) {
+            tma_load_3d(halo_s + slot * Lay::kHaloSlot + Lay::kHaloBoxSlot, &m.delta_halo, bar,
+                        x0 - 4, yy, 0);
+        }
     };
     auto issue_own = [&](int i) {
-        const uint32_t slot = static_cast<uint32_t>(i & 1);
-        const uint32_t bar = bar_s + 16 + 8 * slot;
-        const uint32_t dst = own_s + slot * Lay::kOwnSlot;
-        mbar_arrive_expect_tx(bar, Lay::kOwnTx);
-        tma_load_3d(dst, &m.in_own, bar, x0, y0 + i, 0);
-        if constexpr (STAGE == 2) {
-            tma_load_3d(dst + Lay::kOwnBoxSlot, &m.out_own, bar, x0, y0 + i, 0);
+        if constexpr (Lay::kOwnBoxes > 0) {
+            const uint32_t slot = static_cast<uint32_t>(i & 1);
+            const uint32_t bar = bar_s + 16 + 8 * slot;
+            const uint32_t dst = own_s + slot * Lay::kOwnSlot;
+            mbar_arrive_expect_tx(bar, Lay::kOwnTx);
+            tma_load_3d(dst, &m.in_own, bar, x0, y0 + i, 0);
+            if constexpr (STAGE == 2) {
+                tma_load_3d(dst + Lay::kOwnBOff, &m.out_own, bar, x0, y0 + i, 0);
+            }
         }
     };
     int halo_issued = 0, own_issued = 0, halo_done = 0, own_done = 0;
@@ -130,7 +149,8 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             issue_own(1);
         }
     }
-    halo_issued = own_issued = nrows > 1 ? 2 : 1;
+    halo_issued = nrows > 1 ? 2 : 1;
+    own_issued = Lay::kOwnBoxes > 0 ? halo_issued : 0;
 
     auto load = [&](int y, Raw& r) { Policy::load_raw(a, g, sx, map_index(y, g.ny, g.bc_y), r); };
     // Primitives of this lane's cell of row y. With a mask, an interior solid cell (by its own,
@@ -281,6 +301,10 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
                     rn.v[c] = src[c * kTmaHaloW];
+                    if constexpr (Lay::kHaloBoxes == 2) { // U* hi = fl(hi(U^n) + delta)
+                        rn.v[c] = __fadd_rn(rn.v[c],
+                                            src[Lay::kHaloBoxSlot / sizeof(T) + c * kTmaHaloW]);
+                    }
                 }
             } else {
                 load(y + 2, rn);
@@ -311,12 +335,15 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
         // own-cell operands of row y from the own stream, then the stage update
         {
             const uint32_t slot = static_cast<uint32_t>(i & 1);
-            const bool ok = mbar_wait(bar_s + 16 + 8 * slot, static_cast<uint32_t>((i >> 1) & 1));
-            if (__any_sync(kFull, !ok)) {
-                failed = true;
-                break;
+            if constexpr (Lay::kOwnBoxes > 0) {
+                const bool ok = mbar_wait(bar_s + 16 + 8 * slot,
+                                          static_cast<uint32_t>((i >> 1) & 1));
+                if (__any_sync(kFull, !ok)) {
+                    failed = true;
+                    break;
+                }
+                own_done = i + 1;
             }
-            own_done = i + 1;
             if constexpr (ST > 0) {
                 if (lane == 0) {
                     bulk_wait_read<ST - 1>(); // the store that last used this slot has read it
@@ -324,11 +351,12 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                 __syncwarp();
             }
             const T* src = own_f + slot * (Lay::kOwnSlot / sizeof(T)) + (lane - 2);
-            // own-cell operand q: plane q of the stage input, then (stage 2) of U^n
+            // own-cell operand q: plane q of box A (the stage input; delta in the increment
+            // form), then (stage 2) plane q - kOwnPlanesA of box B (U^n)
             auto op = [&](int q) {
-                return q < kOwnPlanes
+                return q < Lay::kOwnPlanesA
                            ? src[q * kTmaOwnW]
-                           : src[Lay::kOwnBoxSlot / sizeof(T) + (q - kOwnPlanes) * kTmaOwnW];
+                           : src[Lay::kOwnBOff / sizeof(T) + (q - Lay::kOwnPlanesA) * kTmaOwnW];
             };
             const bool solid = MASK && own && is_solid(a.mask, g, gx, y);
             if constexpr (!MASK) {
@@ -400,7 +428,7 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                     issue_own(i + 2);
                 }
             }
-            if (i + 2 < nrows) {
+            if (i + 2 < nrows && Lay::kOwnBoxes > 0) {
                 own_issued = i + 3;
             }
         }
@@ -470,7 +498,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const typename
         static_assert(!MASK || ST == 0, "masked strips store through the lanes");
         smax = march_tma_strip<L, STAGE, LY, HF, ST, NI, MASK, Policy>(
             a, m, x0, static_cast<int>(blockIdx.y) * LY, lane,
-            base + warp * MarchTmaLayout<STAGE, ST, sizeof(typename Policy::T)>::kWarpBytes,
+            base + warp * MarchTmaLayout<STAGE, ST, sizeof(typename Policy::T),
+                                         Policy::kLayout>::kWarpBytes,
             failed);
     }
     if constexpr (STAGE == 2) {

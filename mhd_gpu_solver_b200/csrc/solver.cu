@@ -60,6 +60,8 @@ struct ApiError {
 
 constexpr int kInitThreads = 256;
 constexpr int kGraphBatch = 32;
+// An even batch: a captured batch of increment-form steps ends in the buffer it started from.
+static_assert(kGraphBatch % 2 == 0, "graph batches must hold an even number of steps");
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
@@ -214,8 +216,10 @@ struct mhdb_solver {
     int nxt = 0, nyt = 0;
     size_t ntot = 0;
 
-    void* U = nullptr;  // U^n
-    void* Us = nullptr; // U*
+    void* U = nullptr;  // U^n, the current state
+    void* Us = nullptr; // U*; in the increment form the other state buffer (swapped with U
+                        // after every step)
+    float* delta = nullptr; // increment form: 9 float planes of dt L (allocated on first use)
     double* staging = nullptr;
     uint8_t* mask = nullptr;
     Ctrl* ctrl = nullptr;
@@ -344,6 +348,12 @@ struct StepPlan {
     StageArgsMx b1{}, b2{};
     StageFnMxTma t1 = nullptr, t2 = nullptr; // TMA-fed FP32-mixed kernels (m1/m2 unused then)
     StageFnF64Tma d1 = nullptr, d2 = nullptr; // TMA-fed FP64 kernels (s1/s2 unused then)
+    StageFnDeltaTma e1 = nullptr, e2 = nullptr; // FP32-mixed increment form (m1/m2 unused then)
+    // increment form, by parity q: U^n in buffer q (0: the handle's U at planning time, 1: its
+    // Us), U^{n+1} written to buffer 1 - q
+    StageArgsDelta c1[2]{}, c2[2]{};
+    MarchTmaMaps dm1[2]{}, dm2[2]{};
+    const void* p0 = nullptr;
     MarchTmaMaps tm1{}, tm2{};
     dim3 grid, block;
     size_t smem = 0, smem2 = 0; // dynamic shared memory of stage 1 and stage 2
@@ -412,6 +422,26 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
                 !encode_march_maps(us, u, h->geom, &s.tm2, &err)) {
                 throw ApiError{MHDB_CUDA_ERROR, err};
             }
+        } else if (sk.dx_tma1 != nullptr) {
+            // increment form: the state alternates between the two buffers step by step
+            s.e1 = sk.dx_tma1;
+            s.e2 = sk.dx_tma2;
+            if (h->delta == nullptr) {
+                MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->delta),
+                                      9 * h->geom.plane * sizeof(float)));
+            }
+            const MixedState bufs[2] = {u, us};
+            s.p0 = h->U;
+            for (int q = 0; q < 2; ++q) {
+                s.c1[q] = StageArgsDelta{bufs[q], bufs[1 - q], h->delta, nullptr, h->ctrl,
+                                         h->geom, s.k, h->walls ? 1 : 0};
+                s.c2[q] = s.c1[q];
+                std::string err;
+                if (!encode_march_maps_delta(bufs[q], h->delta, h->geom, &s.dm1[q], &s.dm2[q],
+                                             &err)) {
+                    throw ApiError{MHDB_CUDA_ERROR, err};
+                }
+            }
         }
     }
     if (sk.threads == 0) {
@@ -425,6 +455,9 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     if (s.d1 != nullptr) {
         MHDB_CHECK(cudaFuncSetAttribute(s.d1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
         MHDB_CHECK(cudaFuncSetAttribute(s.d2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
+    } else if (s.e1 != nullptr) {
+        MHDB_CHECK(cudaFuncSetAttribute(s.e1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+        MHDB_CHECK(cudaFuncSetAttribute(s.e2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
     } else if (!s.mixed) {
         MHDB_CHECK(cudaFuncSetAttribute(s.s1, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
         MHDB_CHECK(cudaFuncSetAttribute(s.s2, cudaFuncAttributeMaxDynamicSharedMemorySize, b2));
@@ -443,6 +476,10 @@ void launch_stage(mhdb_solver* h, const StepPlan& s, int stage)
     if (s.d1 != nullptr) {
         (stage == 1 ? s.d1 : s.d2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
             stage == 1 ? s.a1 : s.a2, stage == 1 ? s.tm1 : s.tm2);
+    } else if (s.e1 != nullptr) {
+        const int q = h->U == s.p0 ? 0 : 1;
+        (stage == 1 ? s.e1 : s.e2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
+            stage == 1 ? s.c1[q] : s.c2[q], stage == 1 ? s.dm1[q] : s.dm2[q]);
     } else if (!s.mixed) {
         (stage == 1 ? s.s1 : s.s2)<<<s.grid, s.block, stage == 1 ? s.smem : s.smem2, h->stream>>>(
             stage == 1 ? s.a1 : s.a2);
@@ -479,6 +516,9 @@ void launch_step_direct(mhdb_solver* h, const StepPlan& s)
         } else {
             launch_stage(h, s, stage);
         }
+    }
+    if (s.e1 != nullptr) {
+        std::swap(h->U, h->Us); // the increment form's stage 2 wrote U^{n+1} to the other buffer
     }
 }
 
@@ -626,6 +666,7 @@ void release(mhdb_solver* h)
     }
     if (h->U) cudaFree(h->U);
     if (h->Us) cudaFree(h->Us);
+    if (h->delta) cudaFree(h->delta);
     if (h->staging) cudaFree(h->staging);
     if (h->mask) cudaFree(h->mask);
     if (h->ctrl) cudaFree(h->ctrl);

@@ -69,6 +69,7 @@ struct StageArgsF64 {
 struct PolicyF64 {
     using T = double;
     using Args = StageArgsF64;
+    static constexpr int kLayout = 0; // MarchTmaLayout of the stored form
     struct Raw {
         double v[9];
     };

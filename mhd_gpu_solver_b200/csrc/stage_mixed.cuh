@@ -107,6 +107,7 @@ __device__ __forceinline__ void fast_two_sum(float s, float t, float& h, float& 
 struct PolicyMixed {
     using T = float;
     using Args = StageArgsMx;
+    static constexpr int kLayout = 0; // MarchTmaLayout of the stored form
     struct Raw {
         float v[9];
     };

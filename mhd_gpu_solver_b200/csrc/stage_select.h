@@ -10,6 +10,7 @@
 #include <string>
 
 #include "stage_f64.cuh"
+#include "stage_delta.cuh"
 #include "stage_mixed.cuh"
 #include "tma.cuh"
 
@@ -19,17 +20,25 @@ using StageFnF64 = void (*)(StageArgsF64);
 using StageFnMx = void (*)(StageArgsMx);
 using StageFnMxTma = void (*)(StageArgsMx, MarchTmaMaps); // TMA-fed kernels take tensor maps
 using StageFnF64Tma = void (*)(StageArgsF64, MarchTmaMaps);
+using StageFnDeltaTma = void (*)(StageArgsDelta, MarchTmaMaps); // increment form
 
 struct StageKernels {
     StageFnF64 f64_stage1 = nullptr, f64_stage2 = nullptr;
     StageFnMx mx_stage1 = nullptr, mx_stage2 = nullptr;
     StageFnMxTma mx_tma1 = nullptr, mx_tma2 = nullptr;
     StageFnF64Tma f64_tma1 = nullptr, f64_tma2 = nullptr;
+    StageFnDeltaTma dx_tma1 = nullptr, dx_tma2 = nullptr; // FP32-mixed increment form
     int tile_x = 0, tile_y = 0, threads = 0; // threads == 0: no such configuration
     size_t smem = 0, smem2 = 0;               // dynamic shared memory per block, stage 1 and 2
 };
 
-enum StageKernelKind : int { kKindTile = 0, kKindTileMerged = 1, kKindMarch = 2, kKindMarchTma = 3 };
+enum StageKernelKind : int {
+    kKindTile = 0,
+    kKindTileMerged = 1,
+    kKindMarch = 2,
+    kKindMarchTma = 3,
+    kKindMarchTmaDelta = 4 // TMA strip march of the increment form (stage_delta.cuh)
+};
 
 // tile_x x tile_y: interior cells one block covers (strip march: warps x 28 columns by the rows
 // of a warp's segment).
@@ -56,6 +65,10 @@ bool encode_march_maps(const MixedState& in, const MixedState& out, const Geomet
 // The same for the FP64 state (9 double planes).
 bool encode_march_maps_f64(const double* in, const double* out, const Geometry& g,
                            MarchTmaMaps* maps, std::string* err);
+// Both stages' tensor maps of the increment form: U^n (18 float planes) and the increment
+// (9 float planes).
+bool encode_march_maps_delta(const MixedState& un, float* delta, const Geometry& g,
+                             MarchTmaMaps* stage1, MarchTmaMaps* stage2, std::string* err);
 
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);

@@ -18,11 +18,16 @@ namespace mhdb {
 //   in_halo: stage input, box {kTmaHaloW, 1, 9}    (hi planes of one row, x halo included)
 //   in_own:  stage input, box {kTmaOwnW, 1, 18}    (hi and lo of a warp's owned columns)
 //   out_own: stage output, box {kTmaOwnW, 1, 18}   (stage 2 only: U^n, updated in place)
-// For an FP64 state they span its 9 double planes and every box holds all 9.
+// For an FP64 state they span its 9 double planes and every box holds all 9. In the increment
+// form (stage_delta.cuh) stage 2 reads U* = U^n + delta from two tensors: in_halo is U^n's hi
+// planes, delta_halo the increment's 9 planes (box {kTmaHaloW, 1, 9}), in_own the increment
+// (box {kTmaOwnW, 1, 9}) and out_own U^n's own cells (box {kTmaOwnW, 1, 18}; read, since stage 2
+// writes U^{n+1} to the other state buffer); stage 1 uses in_halo only.
 struct MarchTmaMaps {
     CUtensorMap in_halo;
     CUtensorMap in_own;
     CUtensorMap out_own;
+    CUtensorMap delta_halo;
 };
 
 constexpr int kTmaOwnW = 28;  // owned columns of a warp (a multiple of 4: 16-byte x offsets)

@@ -179,13 +179,24 @@ class DeviceStrip:
         self.dev.set_cell_size((x_max - x_min) / nx, dy)
         self.dev.configure(bc_x, bc_y, mask_rows, walls)
         self.dev.set_reduce_rows(strip.lo, strip.lo + strip.ny)
-        v = self.dev.strip_view()
         self.device = torch.device("cuda", torch.cuda.current_device())
-        dtype = torch.float64 if v.elem_bytes == 8 else torch.float32
-        self.state = _device_tensor(v.state, (v.planes, strip.rows, v.pitch),
-                                    (v.plane, v.pitch, 1), dtype, self.device)
+        v = self.dev.strip_view()
         self.ch = _device_tensor(v.ch_bits, (1,), (1,), torch.int64, self.device)
         self.stream = torch.cuda.ExternalStream(self.dev.stream(), device=self.device)
+        self._ptr = None
+        self._refresh()
+
+    def _refresh(self) -> None:
+        """View of the current state buffer (the FP32-mixed increment form alternates between
+        two buffers step by step)."""
+        import torch
+
+        v = self.dev.strip_view()
+        if v.state != self._ptr:
+            dtype = torch.float64 if v.elem_bytes == 8 else torch.float32
+            self.state = _device_tensor(v.state, (v.planes, self.strip.rows, v.pitch),
+                                        (v.plane, v.pitch, 1), dtype, self.device)
+            self._ptr = v.state
 
     def rows(self, a: int, b: int):
         """All planes of strip rows [a, b), interior columns (a writable view)."""
@@ -193,9 +204,11 @@ class DeviceStrip:
 
     def begin(self, params, nsteps: int) -> None:
         self.dev.strip_begin(params, nsteps)
+        self._refresh()
 
     def step(self) -> None:
         self.dev.strip_step()
+        self._refresh()
 
     def finish(self) -> None:
         self.dev.strip_finish()

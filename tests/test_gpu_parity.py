@@ -417,6 +417,36 @@ def test_default_configuration_of_a_large_grid_matches_fp64():
         assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (kw, err)
 
 
+@pytest.mark.parametrize("case", range(len(MARCH_CASES)))
+@pytest.mark.parametrize("ni", [False, True])
+def test_increment_form_matches_stored_form(case, ni):
+    """The FP32-mixed increment form (stage 1 stores the FP32 increment dt L, stage 2 rebuilds
+    U* = U^n + increment) against the stored form of the same strip-march shape and against the
+    FP64 oracle: within the FP32-mixed tolerance, same step count and clock."""
+    nx, ny, bcx, bcy, state, lim = MARCH_CASES[case]
+    prim = (wl.fourier_state(nx, ny, 9) if state == "fourier" else wl.four_quadrant(nx, ny, 3))
+    bc = (bcx, bcy)
+    U0 = initial_state(prim, 5.0 / 3.0, bc)
+    kw = NI_PARAMS if ni else {}
+    p = orc.Params(limiter=lim, max_steps=25, fixed_steps=True, **kw)
+    ref, tr, sr, _ = orc.solve(U0, orc.Grid(nx, ny), p, bc)
+    cfgs = _capi.tile_configs(_capi.FP32)
+    delta = [c for c in cfgs if c["kind"] == "march_tma_delta"]
+    assert delta
+    for cfg in delta:
+        twin = next(c for c in cfgs if c["kind"] == "march_tma" and c["tile_y"] == cfg["tile_y"]
+                    and c["threads"] == cfg["threads"] and c["min_blocks"] == cfg["min_blocks"])
+        got, tg, sg, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32,
+                              tile_config=cfg["config"])
+        stored, ts, ss, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32,
+                                 tile_config=twin["config"])
+        assert sg == ss == sr
+        assert abs(tg - tr) <= 1e-6 * max(1.0, tr) and abs(tg - ts) <= 1e-6 * max(1.0, ts)
+        for other in (ref, stored):
+            err = rel_l1(got, other)
+            assert np.all(err[[0, 1, 2, 4, 5, 6]] <= MIXED_L1), (cfg, err)
+
+
 @pytest.mark.parametrize("bc", [(orc.OUTFLOW, orc.PERIODIC), (orc.PERIODIC, orc.OUTFLOW)])
 @pytest.mark.parametrize("walls", [True, False])
 @pytest.mark.parametrize("ni", [False, True])

@@ -121,7 +121,8 @@ def test_strip_diagnostics_combine_to_the_whole_grid():
     assert diag["finite"] == want["finite"] is True
 
 
-@pytest.mark.parametrize("precision,tile_config", [(_capi.FP64, 7), (_capi.FP32, 11)])
+@pytest.mark.parametrize("precision,tile_config", [(_capi.FP64, 7), (_capi.FP32, 11),
+                                                   (_capi.FP32, 13)])
 def test_strips_on_the_strip_march(precision, tile_config):
     """Strips on the TMA strip march against the FP64 oracle and the whole grid."""
     n = 512
