@@ -196,10 +196,10 @@ def measured_traffic(kind: str, stage: int, cells: float):
     path = os.path.join(ROOT, "profiles", "stage_traffic.json")
     try:
         with open(path) as f:
-            prof = json.load(f)
-    except (OSError, ValueError):
+            prof = json.load(f)["kinds"].get(kind)
+    except (OSError, ValueError, KeyError):
         return None, None
-    if prof.get("kind") != kind:
+    if prof is None:
         return None, None
     return prof["dram_bytes_per_cell"][f"stage{stage}"] * cells, prof.get("source")
 

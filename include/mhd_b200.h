@@ -175,8 +175,9 @@ int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, i
                           int* min_blocks);
 int mhdb_tile_config_kind(int precision, int config);
 /* mhdb_set_tile_config(h, -1) restores the default: FP32-mixed solves of at least 1024 x 1024
-   cells run the TMA strip march (one warp per block; configuration 11 for masked solves, the TMA
-   strip march that also serves masks), smaller FP32-mixed ones configuration 0; FP64 solves of
+   cells run the TMA strip march (one warp per block; unmasked solves in the increment form,
+   configuration 13; masked ones configuration 11, the TMA strip march that also serves masks),
+   smaller FP32-mixed ones configuration 0; FP64 solves of
    at least 2048 x 2048 cells run the FP64 TMA strip march (configuration 7, which also serves
    masks), smaller ones the 320-thread tile kernel (configuration 2, non-ideal ones configuration
    0), smaller masked FP64 solves configuration 0. */
