@@ -80,11 +80,10 @@ void fill_pair(StageKernels& k)
             k.f64_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                           Policy>;
         } else if constexpr (Cfg::DELTA) {
-            static_assert(!MASK && Cfg::ST1 == 0 && Cfg::ST2 == 0,
-                          "the increment form serves unmasked solves, lane stores");
-            k.dx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+            static_assert(Cfg::ST1 == 0 && Cfg::ST2 == 0, "the increment form stores through the lanes");
+            k.dx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                          PolicyDelta<1>>;
-            k.dx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, false,
+            k.dx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                          PolicyDelta<2>>;
         } else {
             k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;

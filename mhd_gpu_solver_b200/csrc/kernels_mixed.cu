@@ -17,7 +17,7 @@ using Cfg9 = MarchTmaCfg<1, 32, 16>;
 using Cfg10 = MarchTmaCfg<4, 32, 4, true, 0>;
 using Cfg11 = MarchTmaCfg<1, 32, 16, true, 0>;
 using Cfg12 = MarchTmaCfg<1, 64, 16>;
-using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, true>; // increment form
+using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, true>; // increment form (also masked)
 using Cfg14 = MarchTmaCfg<1, 64, 16, true, 0, 0, true>; // increment form, 64-row segments
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
@@ -72,7 +72,7 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
     case 12:
         return select_unmasked<PolicyMixed, Cfg12>(limiter, nonideal, mask);
     case 13:
-        return select_unmasked<PolicyMixed, Cfg13>(limiter, nonideal, mask);
+        return select_full<PolicyMixed, Cfg13>(limiter, nonideal, mask);
     case 14:
         return select_unmasked<PolicyMixed, Cfg14>(limiter, nonideal, mask);
     default:

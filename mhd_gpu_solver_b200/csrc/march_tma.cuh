@@ -77,8 +77,7 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
     using Raw = typename Policy::Raw;
     using Lay = MarchTmaLayout<STAGE, ST, sizeof(T), Policy::kLayout>;
     static_assert(sizeof(T) == 4 || ST == 0, "the FP64 TMA strip march stores through the lanes");
-    static_assert(!Lay::kDelta || (ST == 0 && !MASK),
-                  "the increment form serves unmasked solves and stores through the lanes");
+    static_assert(!Lay::kDelta || ST == 0, "the increment form stores through the lanes");
     constexpr unsigned kFull = 0xffffffffu;
     const Geometry& g = a.geom;
     const Consts& k = a.k;
@@ -368,6 +367,44 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                     T Lz[9] = {};
                     Policy::template update<STAGE, true>(a, g, gx, y, true, Lz, T(0), 0.0, dt,
                                                          k, smax);
+                }
+            } else if constexpr (Lay::kDelta) {
+                if (solid && a.walls) {
+                    // The stored U* of a solid cell is the fill of U^n: stage 1 stores the
+                    // increment fill(U^n) - U^n (rounded to FP32; U^n of the cell from global
+                    // memory, as stage 1 has no own stream); stage 2 stores (U*_stored +
+                    // fill(U*)) / 2 into U^{n+1}, with U*_stored = U^n + increment. The fill is
+                    // this row's filled primitives Wm, made conservative in FP64.
+                    const double rho = Wm[0], vx = Wm[1], vy = Wm[2], vz = Wm[3];
+                    const double bx = Wm[5], by = Wm[6], bz = Wm[7];
+                    double f[9] = {rho, rho * vx, rho * vy, rho * vz,
+                                   static_cast<double>(Wm[4]) * k.inv_gm1 +
+                                       0.5 * rho * (vx * vx + vy * vy + vz * vz) +
+                                       0.5 * (bx * bx + by * by + bz * bz),
+                                   bx, by, bz, static_cast<double>(Wm[8])};
+                    const size_t o = static_cast<size_t>(y) * g.pitch + gx;
+                    if constexpr (STAGE == 1) {
+                        double un[9];
+                        load_cons_mx(a.un, g, gx, y, un);
+#pragma unroll
+                        for (int c = 0; c < 9; ++c) {
+                            a.delta[static_cast<size_t>(c) * g.plane + o] =
+                                __double2float_rn(f[c] - un[c]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 9; ++c) {
+                            const double us = (static_cast<double>(op(9 + c)) +
+                                               static_cast<double>(op(18 + c))) +
+                                              static_cast<double>(op(c));
+                            split_store(a.out, static_cast<size_t>(c) * g.plane + o,
+                                        0.5 * (us + f[c]));
+                        }
+                    }
+                } else if (solid) {
+                    // without walls a solid cell only has L = 0
+                    const T Lz[9] = {};
+                    Policy::template update_ops<STAGE>(a, g, gx, y, true, Lz, dt, k, smax, op);
                 }
             } else if (solid && a.walls) {
                 // L = 0 and the stored value is the wall fill of the stage input (tile kernel:

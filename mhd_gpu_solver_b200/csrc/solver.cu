@@ -433,8 +433,9 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
             const MixedState bufs[2] = {u, us};
             s.p0 = h->U;
             for (int q = 0; q < 2; ++q) {
-                s.c1[q] = StageArgsDelta{bufs[q], bufs[1 - q], h->delta, nullptr, h->ctrl,
-                                         h->geom, s.k, h->walls ? 1 : 0};
+                s.c1[q] = StageArgsDelta{bufs[q], bufs[1 - q], h->delta,
+                                         h->has_mask ? h->mask : nullptr, h->ctrl, h->geom, s.k,
+                                         h->walls ? 1 : 0};
                 s.c2[q] = s.c1[q];
                 std::string err;
                 if (!encode_march_maps_delta(bufs[q], h->delta, h->geom, &s.dm1[q], &s.dm2[q],

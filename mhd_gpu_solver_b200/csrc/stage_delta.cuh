@@ -13,7 +13,9 @@
 // recovery needs them) and writes 9 planes: 72 B per cell instead of 144; stage 2 reads U^n and
 // delta and writes U^{n+1}: 180 B instead of 216. Stage 2's stencil reads U^n of neighbouring
 // cells, so U^{n+1} goes to the other state buffer (the two buffers alternate step by step).
-// Unmasked solves only.
+// With a mask, a solid cell's stored U* is the wall fill of U^n, so stage 1 stores the increment
+// fill(U^n) - U^n rounded to FP32 (the stored form rounds that fill to its FP32 primitives too);
+// the FP64 wall fill reads U^n, or U^n + delta in stage 2, from global memory.
 #pragma once
 
 #include "stage_mixed.cuh"
@@ -24,7 +26,7 @@ struct StageArgsDelta {
     MixedState un;       // U^n: read by both stages
     MixedState out;      // U^{n+1}: written by stage 2 (the other state buffer)
     float* delta;        // 9 planes: fl(dt L) of stage 1 (U* = U^n + delta exactly)
-    const uint8_t* mask; // always nullptr: unmasked solves
+    const uint8_t* mask; // padded fluid mask or nullptr
     Ctrl* ctrl;
     Geometry geom;
     Consts k;
@@ -79,6 +81,18 @@ struct PolicyDelta {
     static __device__ __forceinline__ float signal_speed_f(const float* r, const Consts& k)
     {
         return PolicyMixed::signal_speed_f(r, k);
+    }
+    static __device__ __forceinline__ void prim_of(const double* f, const Consts& k, float* w)
+    {
+        PolicyMixed::prim_of(f, k, w);
+    }
+    // FP64 wall fill of a solid cell from its fluid neighbours' full-precision stage input.
+    template <int S, bool MASK>
+    static __device__ __forceinline__ void wall_fill(const Args& a, const Geometry& g, int x,
+                                                     int y, double gm1, double* out)
+    {
+        wall_fill_any([&](int i, int j, double* s) { full(a, g, i, j, s); }, a.mask, g, x, y,
+                      gm1, out);
     }
     // Stage update of one cell. Stage 1 stores delta = fl(dt L). Stage 2 reads its own-cell
     // operands op(i): delta (i < 9), hi(U^n) (i < 18) and lo(U^n) (i < 27), and stores U^{n+1}.
