@@ -6,8 +6,8 @@ to a power of two, per precision form and limiter) the tuner times each configur
 synthetic smooth state for a few RK2 steps, with CUDA events on the solver's stream, and
 remembers the fastest. Results are cached in memory for the process and can be saved to / loaded
 from a JSON file. Configurations other than 0 serve unmasked solves (the strip-march ones ideal
-and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configuration 11 and
-FP64 configuration 7 also masked solves); a solve that the chosen configuration does not serve runs the library's default
+and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configurations 11 and
+13 and FP64 configuration 7 also masked solves); a solve that the chosen configuration does not serve runs the library's default
 for its size.
 
 ``tune_batch`` does the same for the batched form: per (precision, limiter, ideal or non-ideal,
