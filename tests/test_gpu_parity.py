@@ -230,6 +230,44 @@ def test_resident_continuation_equals_round_trip():
     assert np.all(rel_l1(outs[0], ref) <= FP64_L1)
 
 
+@pytest.mark.parametrize("masked", [False, True])
+def test_increment_form_state_buffers_alternate_correctly(masked):
+    """The increment form writes U^{n+1} to the other state buffer: solves of odd and even step
+    counts in sequence (7, then 40 through a captured 32-step batch and 8 direct steps, then 3)
+    equal a download/upload round trip between them and, without a mask, one 50-step solve (with
+    a mask every solve ends with the reference's wall fill, which the next one starts from), and
+    download, diagnostics and the next solve all see the current buffer."""
+    nx, ny = 150, 96
+    bc = (orc.PERIODIC, orc.OUTFLOW)
+    mask = _edge_mask(nx, ny, 4) if masked else None
+    U0 = initial_state(wl.fourier_state(nx, ny, 8), 5.0 / 3.0, bc, mask)
+    cp = _capi.make_params(limiter=_capi.VANLEER)
+    outs, diags = [], []
+    for plan in ((7, 40, 3), (7, 40, 3, "rt"), (50,)):
+        dev = _capi.DeviceSolver(nx, ny, precision=_capi.FP32)
+        dev.set_tile_config(13)
+        dev.configure(bc[0], bc[1], mask, True)
+        dev.upload(U0)
+        for n in plan:
+            if n == "rt":
+                continue
+            dev.solve_steps(cp, n)
+            if "rt" in plan and n == 7:
+                dev.upload(dev.download())
+        outs.append(dev.download())
+        diags.append(dev.diagnostics(cp))
+        dev.close()
+    assert np.array_equal(outs[0], outs[1])
+    if not masked:
+        assert np.array_equal(outs[0], outs[2])
+        assert diags[0] == diags[2]
+    ref = U0
+    for n in (7, 40, 3):
+        p = orc.Params(limiter=orc.VANLEER, max_steps=n, fixed_steps=True)
+        ref, *_ = orc.solve(ref, orc.Grid(nx, ny), p, bc, mask)
+    assert np.all(rel_l1(outs[0], ref)[[0, 1, 2, 4, 5, 6]] <= MIXED_L1)
+
+
 def test_diagnostics_match_oracle():
     n = 64
     bc = (orc.OUTFLOW, orc.PERIODIC)
