@@ -13,7 +13,9 @@ zone-updates/s (interior cells x steps / device seconds).
   stage 1 reads U and writes U*, 144 B/cell; stage 2 reads U* and U and writes U, 216 B/cell;
   360 B per zone-update) over its average event-timed duration, against the measured HBM copy
   bandwidth; ``traffic`` = that kernel's DRAM bytes per launch from the committed ncu capture of
-  the same kernel kind (profiles/stage_traffic.json, bytes per cell x cells).
+  the same kernel kind (profiles/stage_traffic.json, bytes per cell x cells). The FP32-mixed
+  increment form moves fewer bytes (72 and 180 B/cell, ``form_bytes_per_launch``); the fraction
+  is still taken on the canonical bytes.
 * ``cpu_baseline``: the reference CPU solver (SIMD + threads), compiled from the reference's
   own headers into oracle/_ref, on all host cores, on a bounded number of steps of the same
   4096^2 state (MC limiter: the reference has no van Leer).
@@ -47,6 +49,9 @@ SEED = 0
 GAMMA = 5.0 / 3.0
 E2E_STEPS = 500
 BYTES_STAGE = {1: 144.0, 2: 216.0}  # algorithmic bytes per interior cell per launch
+# bytes per interior cell a stage of the FP32-mixed increment form moves (it stores the FP32
+# increment instead of U*); the roofline still divides the canonical BYTES_STAGE by the time
+BYTES_FORM = {"march_tma_delta": {1: 72.0, 2: 180.0}}
 
 
 def parse():
@@ -620,6 +625,8 @@ def main():
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
                      "traffic_source": traffic_src,
                      "algorithmic_bytes_per_launch": BYTES_STAGE[dom] * n * n,
+                     "form_bytes_per_launch": (BYTES_FORM[mixed_cfg["kind"]][dom] * n * n
+                                               if mixed_cfg["kind"] in BYTES_FORM else None),
                      "stage1_avg_ms": mixed["stage1_avg_ms"],
                      "stage2_avg_ms": mixed["stage2_avg_ms"]},
         "clocks": mixed["clocks"],
