@@ -421,7 +421,7 @@ def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
             dev.configure(_capi.BC_OUTFLOW, _capi.BC_PERIODIC, mask, True)
             dev.generate(_capi.InitSpec.fourier(seed), params)
             d0 = dev.diagnostics(params)
-            dev.solve_steps(params, 2)  # warm-up (kernel attributes, graph capture)
+            dev.solve_steps(params, 40)  # warm-up: kernel attributes, the 32-step graph batch
             dev.generate(_capi.InitSpec.fourier(seed), params)
             stream = torch.cuda.ExternalStream(dev.stream())
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
