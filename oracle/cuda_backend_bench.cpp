@@ -1,5 +1,5 @@
-// Timing driver for a CUDA backend of the reference's DeviceSolver interface — BASELINE
-// INFRASTRUCTURE ONLY (it measures; nothing in the product calls it).
+// Timing driver for a CUDA backend of the reference's DeviceSolver interface: same-box
+// comparison infrastructure only (it measures; nothing in the product calls it).
 //
 // oracle/build_oracle.py compiles it from the reference's own, unmodified headers where they lie
 // twice: linked with the reference's own CUDA backend (src/cuda/cuda_solver.cu, nvcc for

@@ -1,7 +1,7 @@
 """CUDA backend (through the C ABI) against the CPU oracle and the reference fixtures.
 
 Tolerances: the plain FP64 form must match the oracle to relative L1 <= 1e-12 per conserved
-component after the stated step count, with the same step count, and the
+component after the stated step count, with the same step count (the FP64 parity bar), and the
 mask must be handled the same way. Components whose reference value is identically zero are
 compared in absolute L1. The FP32-mixed form is held to relative L1 <= 1e-6.
 """
