@@ -125,3 +125,15 @@ def test_host_state_preparation_without_device():
         s.set_backend("cpu")
     with pytest.raises(ValueError, match="Unknown backend"):
         s.set_backend("tpu")
+
+
+def test_bench_traffic_lookup_covers_every_march_tma_kind():
+    """The bench's roofline traffic comes from the committed ncu figure of the dominant kernel's
+    kind: both TMA strip-march forms have one, scaled by cells; other kinds report none."""
+    import bench
+
+    for kind, s2 in (("march_tma", 215.1), ("march_tma_delta", 186.4)):
+        traffic, src = bench.measured_traffic(kind, 2, 1000.0)
+        assert traffic == pytest.approx(s2 * 1000.0) and src
+    assert bench.measured_traffic("tile", 2, 1000.0) == (None, None)
+    assert bench.BYTES_FORM["march_tma_delta"] == {1: 72.0, 2: 180.0}
