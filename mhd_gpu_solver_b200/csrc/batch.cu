@@ -113,6 +113,17 @@ struct LoadMx {
     Geometry g;
     __device__ void operator()(int x, int y, double* v) const { load_cons_mx(u, g, x, y, v); }
 };
+// State of an increment-form solve: buffer (steps & 1) of its step counter, read on the device
+// when the copy runs.
+struct LoadMxParity {
+    MixedState u0, u1;
+    Geometry g;
+    const Ctrl* ctrl;
+    __device__ void operator()(int x, int y, double* v) const
+    {
+        load_cons_mx((ctrl->steps & 1) != 0 ? u1 : u0, g, x, y, v);
+    }
+};
 
 template <int NT, class Load, class Speed>
 __global__ void batch_cfl_init(Load load, Speed speed, Geometry g, Consts k, Ctrl* ctrl)
@@ -211,31 +222,40 @@ struct BatchKernels<PolicyF64> {
 //      through TMA row stores, stage 2 through plain stores;
 //   1: register strip march (rows loaded by the lanes, no shared-memory staging), 4 warps
 //      (112 columns x 32 rows) per item, 4 blocks per SM;
-//   2: as 0 with 64 rows per item.
+//   2: as 0 with 64 rows per item;
+//   3: as 0 in the increment form (stage_delta.cuh): stage 1 stores the FP32 increment, stage 2
+//      writes U^{n+1} to the other state buffer (per-solve buffer parity from its step counter).
 template <>
 struct BatchKernels<PolicyMixed> {
     using Desc = BatchSolveTma;
     using Fn = void (*)(const Desc*, const int2*, int);
-    static constexpr int kVariants = 3;
+    static constexpr int kVariants = 4;
+    static constexpr int kDeltaVariant = 3;
     static BatchVariant variant(int v)
     {
         if (v == 1) return {4 * kMarchOwned, 32, 128, MHDB_KERNEL_MARCH};
         if (v == 2) return {kMarchOwned, 64, 32, MHDB_KERNEL_MARCH_TMA};
+        if (v == 3) return {kMarchOwned, 32, 32, MHDB_KERNEL_MARCH_TMA_DELTA};
         return {kMarchOwned, 32, 32, MHDB_KERNEL_MARCH_TMA};
     }
     // Small solves have too few strips to fill the GPU on their own; their per-item set-up is
-    // cheaper in the register march.
-    static int default_variant(long long cells) { return cells >= 128LL * 128 ? 0 : 1; }
+    // cheaper in the register march. Larger ones run the increment form.
+    static int default_variant(long long cells) { return cells >= 128LL * 128 ? 3 : 1; }
     template <int L, bool NI, int STAGE>
     static Fn fn(int v)
     {
         if (v == 1) return batch_march_kernel<PolicyMixed, L, NI, STAGE, 32, 4, 4, BatchSolveTma>;
         if (v == 2) return batch_march_tma_kernel<L, NI, STAGE, 64, 1, 16, true, (STAGE == 1 ? 1 : 0)>;
+        if (v == 3) return batch_march_delta_kernel<L, NI, STAGE, 32, 1, 16, true>;
         return batch_march_tma_kernel<L, NI, STAGE, 32, 1, 16, true, (STAGE == 1 ? 1 : 0)>;
     }
     static size_t smem(int v, bool, int stage)
     {
         if (v == 1) return 0;
+        if (v == 3) {
+            return stage == 1 ? march_tma_smem_bytes<1, 0, 4, 1>(1)
+                              : march_tma_smem_bytes<2, 0, 4, 1>(1);
+        }
         return stage == 1 ? march_tma_smem_bytes<1, 1>(1) : march_tma_smem_bytes<2, 0>(1);
     }
 };
@@ -275,6 +295,13 @@ struct SolveRec {
     bool fixed = false;
     Ctrl last{}; // host copy after the last poll
     MarchTmaMaps maps[2]{}; // FP32-mixed: tensor maps of stage 1 and stage 2
+    // increment form (FP32-mixed variant 3): the increment planes, the tensor maps of both
+    // buffer parities, whether the solve uses it, and whether it has been stepped (after which
+    // it can no longer change between the stored and the increment form)
+    float* delta = nullptr;
+    MarchTmaMaps dmaps[2][2]{};
+    bool alternates = false;
+    bool stepped = false;
 };
 
 } // namespace
@@ -403,6 +430,34 @@ void rebuild(mhdb_batch* b)
             d.stage[1] = StageArgsMx{us, u, nullptr, ctrl, s.geom, s.k, 1};
             d.maps[0] = s.maps[0];
             d.maps[1] = s.maps[1];
+            const bool alt = s.variant == BatchKernels<PolicyMixed>::kDeltaVariant;
+            if (!s.stepped) {
+                s.alternates = alt;
+            }
+            if (s.alternates) {
+                if (s.delta == nullptr) {
+                    const size_t db = 9 * s.geom.plane * sizeof(float);
+                    check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s.delta), db, b->pool,
+                                                  b->stream), "cudaMallocFromPoolAsync(delta)");
+                    b->bytes_in_use += db;
+                    s.bytes += db;
+                    const MixedState bufs[2] = {u, us};
+                    for (int q = 0; q < 2; ++q) {
+                        std::string err;
+                        if (!encode_march_maps_delta(bufs[q], s.delta, s.geom, &s.dmaps[q][0],
+                                                     &s.dmaps[q][1], &err)) {
+                            throw BatchFail{MHDB_CUDA_ERROR, err};
+                        }
+                    }
+                }
+                const MixedState bufs[2] = {u, us};
+                for (int q = 0; q < 2; ++q) {
+                    d.dstage[q] = StageArgsDelta{bufs[q], bufs[1 - q], s.delta, nullptr, ctrl,
+                                                 s.geom, s.k, 1};
+                    d.dmaps[q][0] = s.dmaps[q][0];
+                    d.dmaps[q][1] = s.dmaps[q][1];
+                }
+            }
         }
         d.tiles_x = s.tiles_x;
         d.ntiles = s.tiles_x * s.tiles_y;
@@ -488,6 +543,11 @@ void run_steps(mhdb_batch* b, int nsteps)
     }
     if (b->lists.empty() || nsteps <= 0) {
         return;
+    }
+    for (auto& s : b->solves) {
+        if (s.live && s.last.finished == 0) {
+            s.stepped = true;
+        }
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
@@ -617,6 +677,7 @@ void mhdb_batch_destroy(mhdb_batch* b)
         if (s.live) {
             cudaFreeAsync(s.U, b->stream);
             cudaFreeAsync(s.Us, b->stream);
+            if (s.delta) cudaFreeAsync(s.delta, b->stream);
         }
     }
     cudaStreamSynchronize(b->stream);
@@ -833,6 +894,9 @@ int mhdb_batch_remove(mhdb_batch* b, int id)
         SolveRec& s = b->solves[id];
         check(cudaFreeAsync(s.U, b->stream), "cudaFreeAsync(U)");
         check(cudaFreeAsync(s.Us, b->stream), "cudaFreeAsync(U*)");
+        if (s.delta) {
+            check(cudaFreeAsync(s.delta, b->stream), "cudaFreeAsync(delta)");
+        }
         b->bytes_in_use -= s.bytes;
         b->free_slots.push_back(s.slot);
         s = SolveRec{};
@@ -893,8 +957,19 @@ int mhdb_batch_set_config(mhdb_batch* b, int id, int config)
         if (config < -1 || config >= mhdb_batch_config_count(b->precision)) {
             throw BatchFail{MHDB_INVALID_ARGUMENT, "unknown batch configuration"};
         }
-        if (b->solves[id].config != config) {
-            b->solves[id].config = config;
+        SolveRec& s = b->solves[id];
+        if (b->precision == MHDB_FP32 && s.stepped) {
+            using K = BatchKernels<PolicyMixed>;
+            const int v = config >= 0 ? config
+                                      : K::default_variant(static_cast<long long>(s.grid.nx) * s.grid.ny);
+            if ((v == K::kDeltaVariant) != s.alternates) {
+                throw BatchFail{MHDB_INVALID_ARGUMENT,
+                                "a solve that has been stepped cannot change between the stored "
+                                "and the increment form"};
+            }
+        }
+        if (s.config != config) {
+            s.config = config;
             b->dirty = true;
         }
     });
@@ -978,6 +1053,11 @@ int mhdb_batch_download(mhdb_batch* b, int id, double* const comps[9], size_t n_
         if (b->precision == MHDB_FP64) {
             batch_pack<<<blocks_for(n, 256), 256, 0, st>>>(
                 LoadF64{static_cast<const double*>(s.U), s.geom}, stg, s.geom, s.grid.ng, nxt, nyt, n_tot);
+        } else if (s.alternates) {
+            batch_pack<<<blocks_for(n, 256), 256, 0, st>>>(
+                LoadMxParity{mixed_view(s.U, s.geom), mixed_view(s.Us, s.geom), s.geom,
+                             b->ctrl + s.slot},
+                stg, s.geom, s.grid.ng, nxt, nyt, n_tot);
         } else {
             batch_pack<<<blocks_for(n, 256), 256, 0, st>>>(
                 LoadMx{mixed_view(s.U, s.geom), s.geom}, stg, s.geom, s.grid.ng, nxt, nyt, n_tot);

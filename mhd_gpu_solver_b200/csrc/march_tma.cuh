@@ -24,6 +24,7 @@
 #pragma once
 
 #include "march_kernel.cuh"
+#include "stage_delta.cuh"
 #include "stage_mixed.cuh"
 #include "tma.cuh"
 
@@ -544,10 +545,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) march_tma_kernel(const typename
     }
 }
 
-// One solve of a TMA batch: stage arguments, the tensor maps of both stages, its tiling.
+// One solve of a TMA batch: stage arguments, the tensor maps of both stages, its tiling. For the
+// increment form (stage_delta.cuh) the arguments and maps of both state-buffer parities: parity
+// q holds U^n in buffer q (0: U, 1: U*'s buffer), and a solve that has run s steps is in parity
+// s & 1.
 struct BatchSolveTma {
     MarchTmaMaps maps[2]; // stage 1 and stage 2
     StageArgsMx stage[2];
+    MarchTmaMaps dmaps[2][2]; // increment form: [parity][stage - 1]
+    StageArgsDelta dstage[2]; // increment form: [parity]
     int tiles_x; // blocks per row
     int ntiles;  // blocks of this solve
 };
@@ -598,6 +604,65 @@ __global__ void __launch_bounds__(NW * 32, MINB) batch_march_tma_kernel(
             }
             __syncwarp();
             smax = march_tma_strip<L, STAGE, LY, HF, ST, NI>(sa, m, x0, y0, lane, wbase, failed);
+        }
+        if constexpr (STAGE == 2) {
+            reduce_signal_speed_and_finish(smax, sa.ctrl, sa.k, static_cast<unsigned>(s_ntiles),
+                                           true);
+        }
+    }
+}
+
+// The batch kernel of the increment form: as batch_march_tma_kernel, with each solve's
+// arguments and tensor maps taken for the state-buffer parity of its step counter (read before
+// the stage; it only changes when the solve's stage-2 reduction completes).
+template <int L, bool NI, int STAGE, int LY, int NW, int MINB, bool HF>
+__global__ void __launch_bounds__(NW * 32, MINB) batch_march_delta_kernel(
+    const BatchSolveTma* solves, const int2* __restrict__ work, int nwork)
+{
+    __shared__ __align__(16) StageArgsDelta sa;
+    __shared__ int s_tiles_x, s_ntiles, s_q;
+    extern __shared__ unsigned char march_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = march_smem + ((128u - (smem_addr(march_smem) & 127u)) & 127u);
+    unsigned char* wbase = base + warp * MarchTmaLayout<STAGE, 0, 4, 1>::kWarpBytes;
+    bool failed = false;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 it = work[w];
+        __syncthreads(); // the previous item is done with sa
+        if (threadIdx.x == 0) {
+            s_q = solves[it.x].dstage[0].ctrl->steps & 1;
+            s_tiles_x = solves[it.x].tiles_x;
+            s_ntiles = solves[it.x].ntiles;
+        }
+        __syncthreads();
+        {
+            const int* src = reinterpret_cast<const int*>(&solves[it.x].dstage[s_q]);
+            int* dst = reinterpret_cast<int*>(&sa);
+            for (int i = threadIdx.x; i < static_cast<int>(sizeof(StageArgsDelta) / sizeof(int));
+                 i += NW * 32) {
+                dst[i] = src[i];
+            }
+        }
+        __syncthreads();
+        if (sa.ctrl->finished != 0) {
+            continue;
+        }
+        const MarchTmaMaps& m = solves[it.x].dmaps[s_q][STAGE - 1];
+        const int x0 = ((it.y % s_tiles_x) * NW + warp) * kMarchOwned;
+        const int y0 = (it.y / s_tiles_x) * LY;
+        double smax = 0.0;
+        if (x0 < sa.geom.nx && !failed) { // warp-uniform
+            if (lane == 0) {
+                tensormap_acquire(&m.in_halo);
+                if constexpr (STAGE == 2) {
+                    tensormap_acquire(&m.in_own);
+                    tensormap_acquire(&m.out_own);
+                    tensormap_acquire(&m.delta_halo);
+                }
+            }
+            __syncwarp();
+            smax = march_tma_strip<L, STAGE, LY, HF, 0, NI, false, PolicyDelta<STAGE>>(
+                sa, m, x0, y0, lane, wbase, failed);
         }
         if constexpr (STAGE == 2) {
             reduce_signal_speed_and_finish(smax, sa.ctrl, sa.k, static_cast<unsigned>(s_ntiles),

@@ -217,6 +217,46 @@ def test_launch_poll_and_downloads_beside_running_steps():
         assert np.array_equal(got[sid], ref)
 
 
+def test_increment_form_batch_with_odd_step_counts():
+    """Batch configuration 3 (increment form: each solve's state alternates between its two
+    buffers, the parity taken from its own step counter) with odd and even step counts, finished
+    solves downloaded while the others still step: the same values as the stored form
+    (configuration 0) within the FP32-mixed tolerance. A stepped solve cannot switch between the
+    two forms; other changes stay open."""
+    steps = [13, 20, 27]
+    cases = [CASES[0], CASES[1], CASES[4]]
+    states = [state(c[0], c[1], 70 + i, c[2], c[3], c[6]) for i, c in enumerate(cases)]
+    outs = {}
+    for cfg in (0, 3):
+        b = BatchSolver(_capi.FP32)
+        ids = []
+        for U, n, c in zip(states, steps, cases):
+            sid = b.add(U, fixed_params(n, **params_of(c)), c[3], fixed_steps=True)
+            b.set_config(sid, cfg)
+            ids.append(sid)
+        got, active = {}, len(ids)
+        while active > 0:
+            b.launch(5)
+            active = b.poll()
+            for sid in ids:
+                if sid not in got and b.status(sid)[1]:
+                    got[sid] = b.download(sid)
+        for sid, n in zip(ids, steps):
+            assert b.status(sid)[0].steps == n
+        outs[cfg] = [got[i] for i in ids]
+        if cfg == 3:
+            live = b.add(states[0], fixed_params(9, **params_of(cases[0])), cases[0][3],
+                         fixed_steps=True)
+            b.set_config(live, 3)
+            b.step(1)
+            with pytest.raises(_capi.MhdbValueError):
+                b.set_config(live, 0)
+            b.set_config(live, 3)
+        b.close()
+    for a, c in zip(outs[0], outs[3]):
+        assert np.all(rel_l1(c, a)[[0, 1, 2, 4, 5, 6]] <= 1e-6)
+
+
 def test_every_batch_configuration_gives_the_same_values():
     """The FP32-mixed batch configurations (TMA strip march with 32- or 64-row items, register
     strip march) run the same arithmetic and agree to FP32 rounding (the compiler may contract
