@@ -264,9 +264,12 @@ int mhdb_batch_poll(mhdb_batch* b, int* active);
    threads per work item). mhdb_batch_config_info writes the interior cells of one work item
    (tile width and height), its threads and its kernel kind (MHDB_KERNEL_*). FP32-mixed: 0 = TMA
    strip march, one warp by 32 rows; 1 = register strip march, 4 warps by 32 rows; 2 = TMA strip
-   march, one warp by 64 rows. mhdb_batch_set_config picks one for a solve (-1: by the solve's
-   size, the default); the batch autotuner (mhd_gpu_solver_b200.autotune.tune_batch) chooses per
-   size class. The configurations agree to the FP32 rounding of the form. */
+   march, one warp by 64 rows; 3 = TMA strip march of the increment form, one warp by 32 rows
+   (the default for solves of at least 128 x 128 cells; smaller ones take 1).
+   mhdb_batch_set_config picks one for a solve (-1: by the solve's size, the default); once a
+   solve has been stepped it cannot change between configuration 3 and the others
+   (MHDB_INVALID_ARGUMENT). The batch autotuner (mhd_gpu_solver_b200.autotune.tune_batch) chooses
+   per size class. The configurations agree to the FP32 rounding of the form. */
 int mhdb_batch_config_count(int precision);
 int mhdb_batch_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                            int* kind);
