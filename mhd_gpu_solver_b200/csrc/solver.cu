@@ -220,6 +220,10 @@ struct mhdb_solver {
     void* Us = nullptr; // U*; in the increment form the other state buffer (swapped with U
                         // after every step)
     float* delta = nullptr; // increment form: 9 float planes of dt L (allocated on first use)
+    // increment form: parity of the host-side buffer swaps since the solve started. Steps
+    // launched after the solve finished do nothing on the device, so at the end the state is in
+    // the buffer of the parity of the steps actually taken (settle_buffers).
+    int swap_parity = 0;
     double* staging = nullptr;
     uint8_t* mask = nullptr;
     Ctrl* ctrl = nullptr;
@@ -235,9 +239,11 @@ struct mhdb_solver {
     double last_gm1 = 2.0 / 3.0;
     bool solved_since_upload = false;
 
-    // graph cache for a batch of kGraphBatch steps
-    cudaGraphExec_t graph_exec = nullptr;
-    std::vector<double> graph_key;
+    // graph cache for a batch of kGraphBatch steps: two entries, so that the increment form
+    // (whose current state buffer alternates with odd step counts) keeps a graph per buffer
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    std::vector<double> graph_key[2];
+    int graph_next = 0; // entry to replace next
 
     int tile_config = -1; // index into the compiled tile configurations (-1: by grid size)
     bool profiling = false;
@@ -520,7 +526,18 @@ void launch_step_direct(mhdb_solver* h, const StepPlan& s)
     }
     if (s.e1 != nullptr) {
         std::swap(h->U, h->Us); // the increment form's stage 2 wrote U^{n+1} to the other buffer
+        h->swap_parity ^= 1;
     }
+}
+
+// After an increment-form solve: point U at the buffer that holds the state after the steps the
+// device actually took (the Ctrl block read back by read_ctrl).
+void settle_buffers(mhdb_solver* h, const StepPlan& s)
+{
+    if (s.e1 != nullptr && h->swap_parity != (h->ctrl_host->steps & 1)) {
+        std::swap(h->U, h->Us);
+    }
+    h->swap_parity = 0;
 }
 
 // Identity of a captured batch: everything a stage launch depends on, field by field (no
@@ -551,10 +568,18 @@ void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n
         return;
     }
     const std::vector<double> key = plan_key(h, p, s);
-    if (h->graph_exec == nullptr || key != h->graph_key) {
-        if (h->graph_exec != nullptr) {
-            cudaGraphExecDestroy(h->graph_exec);
-            h->graph_exec = nullptr;
+    int e = -1;
+    for (int j = 0; j < 2; ++j) {
+        if (h->graph_exec[j] != nullptr && h->graph_key[j] == key) {
+            e = j;
+        }
+    }
+    if (e < 0) {
+        e = h->graph_next;
+        h->graph_next ^= 1;
+        if (h->graph_exec[e] != nullptr) {
+            cudaGraphExecDestroy(h->graph_exec[e]);
+            h->graph_exec[e] = nullptr;
         }
         cudaGraph_t graph = nullptr;
         MHDB_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -567,17 +592,17 @@ void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n
         if (cap != cudaSuccess) {
             throw CudaFail{cap, "cudaStreamEndCapture"};
         }
-        const cudaError_t ins = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+        const cudaError_t ins = cudaGraphInstantiate(&h->graph_exec[e], graph, 0);
         cudaGraphDestroy(graph);
         if (ins != cudaSuccess) {
-            h->graph_exec = nullptr;
+            h->graph_exec[e] = nullptr;
             throw CudaFail{ins, "cudaGraphInstantiate"};
         }
-        h->graph_key = key;
+        h->graph_key[e] = key;
     }
     const int batches = n / kGraphBatch;
     for (int b = 0; b < batches; ++b) {
-        MHDB_CHECK(cudaGraphLaunch(h->graph_exec, h->stream));
+        MHDB_CHECK(cudaGraphLaunch(h->graph_exec[e], h->stream));
         h->launches += 2 * kGraphBatch;
     }
     for (int i = 0; i < n - batches * kGraphBatch; ++i) {
@@ -601,6 +626,7 @@ void start_solve(mhdb_solver* h, const StepPlan& s, double t_end, int max_steps,
     c.status = 0;
     c.defer = defer;
     *h->ctrl_host = c;
+    h->swap_parity = 0;
     MHDB_CHECK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice,
                                h->stream));
     const long long ncell = static_cast<long long>(h->grid.nx) * h->grid.ny;
@@ -660,7 +686,9 @@ int guarded(mhdb_solver* h, F&& f)
 
 void release(mhdb_solver* h)
 {
-    if (h->graph_exec != nullptr) cudaGraphExecDestroy(h->graph_exec);
+    for (auto& g : h->graph_exec) {
+        if (g != nullptr) cudaGraphExecDestroy(g);
+    }
     for (auto& e : h->prof_pool) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -766,6 +794,7 @@ int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result
                 batch = std::clamp(est, 1, 256);
             }
         }
+        settle_buffers(h, s);
         collect_result(h, fixed_steps < 0, p->t_end, r);
     });
 }
@@ -1270,8 +1299,9 @@ int mhdb_strip_end(mhdb_solver* h, mhdb_result* result)
         if (result == nullptr) {
             throw ApiError{MHDB_INVALID_ARGUMENT, "result must not be NULL"};
         }
-        h->strip.reset();
         read_ctrl(h);
+        settle_buffers(h, *h->strip);
+        h->strip.reset();
         collect_result(h, !h->strip_fixed, h->strip_t_end, result);
     });
 }

@@ -268,6 +268,30 @@ def test_increment_form_state_buffers_alternate_correctly(masked):
     assert np.all(rel_l1(outs[0], ref)[[0, 1, 2, 4, 5, 6]] <= MIXED_L1)
 
 
+def test_increment_form_time_based_solves():
+    """Time-based solves (batches of steps between polls, graph batches and odd remainders) on
+    the increment form, twice in a row on resident state: the oracle's step counts and clock,
+    values within the FP32-mixed tolerance."""
+    nx, ny = 150, 96
+    bc = (orc.PERIODIC, orc.PERIODIC)
+    U0 = initial_state(wl.fourier_state(nx, ny, 3), 5.0 / 3.0, bc)
+    dev = _capi.DeviceSolver(nx, ny, precision=_capi.FP32)
+    ref = U0
+    try:
+        dev.set_tile_config(13)
+        dev.configure(bc[0], bc[1])
+        dev.upload(U0)
+        for t_end in (0.021, 0.0137):
+            r = dev.solve(_capi.make_params(t_end=t_end, limiter=_capi.VANLEER))
+            p = orc.Params(t_end=t_end, limiter=orc.VANLEER)
+            ref, tr, sr, _ = orc.solve(ref, orc.Grid(nx, ny), p, bc)
+            assert r.steps == sr and abs(r.t - tr) <= 1e-6 * tr
+        got = dev.download()
+    finally:
+        dev.close()
+    assert np.all(rel_l1(got, ref)[[0, 1, 2, 4, 5, 6]] <= MIXED_L1)
+
+
 def test_diagnostics_match_oracle():
     n = 64
     bc = (orc.OUTFLOW, orc.PERIODIC)
