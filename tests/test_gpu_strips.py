@@ -92,13 +92,16 @@ def test_strips_match_oracle_and_whole_grid(name, nx, ny, bc, masked, ni, count,
     assert abs(res[0] - wt) <= 1e-12 * wt and abs(res[2] - wc_h) <= TOL[precision] * wc_h
 
 
-def test_time_based_strips_stop_with_the_whole_grid():
+@pytest.mark.parametrize("precision,tile_config", [(_capi.FP64, -1), (_capi.FP32, 13)])
+def test_time_based_strips_stop_with_the_whole_grid(precision, tile_config):
+    """Time-based strip solves (the host steps in batches and may launch steps past the end,
+    which do nothing on the device), also on the increment form whose state buffers alternate."""
     bc = (orc.OUTFLOW, orc.OUTFLOW)
     grid, p, U0, mask = _case(48, 64, bc, True, False, steps=0, t_end=0.01)
-    got, res, _ = _split(grid, p, U0, bc, mask, 2, _capi.FP64)
+    got, res, _ = _split(grid, p, U0, bc, mask, 2, precision, tile_config)
     want, t, steps, c_h = orc.solve(U0, grid, p, bc, mask)
-    assert res[1] == steps and abs(res[0] - t) <= 1e-12 * t
-    check(got, interior(want), c_h, _capi.FP64)
+    assert res[1] == steps and abs(res[0] - t) <= TOL[precision] * t
+    check(got, interior(want), c_h, precision)
 
 
 def test_strip_diagnostics_combine_to_the_whole_grid():
