@@ -67,6 +67,15 @@ constexpr size_t march_tma_smem_bytes(int warps)
     return static_cast<size_t>(warps) * MarchTmaLayout<STAGE, ST, ELEM, KIND>::kWarpBytes + 128;
 }
 
+// The FP32-mixed one-warp configurations run 16 blocks per SM: their shared memory (plus the
+// 1 KB an SM reserves per block) must fit the SM's 228 KB, or occupancy drops.
+constexpr bool fits_16_blocks(size_t bytes) { return 16 * (bytes + 1024) <= 228 * 1024; }
+static_assert(fits_16_blocks(march_tma_smem_bytes<1, 1>(1)) &&
+                  fits_16_blocks(march_tma_smem_bytes<2, 0>(1)) &&
+                  fits_16_blocks(march_tma_smem_bytes<1, 0, 4, 1>(1)) &&
+                  fits_16_blocks(march_tma_smem_bytes<2, 0, 4, 1>(1)),
+              "a one-warp FP32-mixed strip-march layout no longer fits 16 blocks per SM");
+
 template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false,
           class Policy = PolicyMixed>
 __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a,

@@ -53,3 +53,17 @@ def test_argument_errors_before_any_device_work():
     assert _capi.lib.mhdb_precision(None) == -1
     assert _capi.lib.mhdb_launch_count(None) == 0
     _capi.lib.mhdb_destroy(None)
+
+
+def test_kernel_kind_names_match_the_header():
+    """MHDB_KERNEL_* values in include/mhd_b200.h and the names the Python layer gives them."""
+    import os
+    import re
+
+    from mhd_gpu_solver_b200 import _capi
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(root, "include", "mhd_b200.h")) as f:
+        text = f.read()
+    kinds = {int(v): k for k, v in re.findall(r"MHDB_KERNEL_(\w+) = (\d+)", text)}
+    assert {v: n.lower() for v, n in kinds.items()} == _capi.KERNEL_KINDS
