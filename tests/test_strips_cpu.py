@@ -242,7 +242,8 @@ def _rank(rank, world, port, case, per_rank, q):
 @pytest.mark.timeout(240)
 @pytest.mark.parametrize("case,world,per_rank", [("periodic_quadrants", 2, 1),
                                                  ("outflow_masked_nonideal", 2, 2),
-                                                 ("outflow_time_based", 3, 1)])
+                                                 ("outflow_time_based", 3, 1),
+                                                 ("periodic_quadrants", 4, 1)])
 def test_gloo_ranks_equal_whole_grid(case, world, per_rank):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
