@@ -4,6 +4,9 @@
   (MHDSolver, SolveParams, NonIdealConfig, ...) running on the CUDA backend.
 * ``mhd_gpu_solver_b200._capi``: ctypes binding of the C ABI (include/mhd_b200.h).
 * ``mhd_gpu_solver_b200.workloads``: seeded synthetic initial states and masks.
+* ``mhd_gpu_solver_b200.batch`` / ``serve``: many solves in one persistent step, and the
+  continuous-batching request loop over it; ``autotune``: per-size-class configuration choice.
+* ``mhd_gpu_solver_b200.strips``: one grid split into y strips over several GPUs or solvers.
 
 Importing the package loads ``libmhd_b200.so``; there is no CPU fallback, so the import fails
 with ImportError when the library has not been built.
@@ -11,4 +14,4 @@ with ImportError when the library has not been built.
 
 from . import _capi  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
 
-__all__ = ["_capi", "mhd_solver", "workloads"]
+__all__ = ["_capi", "autotune", "batch", "mhd_solver", "serve", "strips", "workloads"]
