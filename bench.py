@@ -7,8 +7,13 @@ zone-updates/s (interior cells x steps / device seconds).
 * ``value``: FP32-mixed form, state resident in HBM, K timed steps bracketed by CUDA events on
   the solver's stream after W warm-up steps. The state (1.2 GB) is far larger than L2 (126 MB),
   so no flush is needed between steps. ``fp64`` reports the plain FP64 form the same way.
-* ``e2e``: the same metric through the C ABI the way a caller uses it (MHDSolver.run): per call,
-  upload from pinned host memory, 500 RK2 steps, download to pinned host memory.
+* ``e2e``: the same metric through the C ABI the way a caller uses it: per call, upload from
+  pinned host memory, 500 RK2 steps, download to pinned host memory (bytes per step = the
+  state's bytes / 500). ``e2e_dropin``: through the reference's own route, its Python module's
+  MHDSolver.run with set_backend("cuda", "fp32") (MC: the module has no van Leer).
+* ``fp64_mc``: the plain FP64 form with the MC limiter on the same state, the like-for-like pair
+  of the reference CPU solver. ``l1_fp32_mixed_vs_fp64``: the FP32-mixed result against the FP64
+  result after 500 steps of the headline state, every component.
 * ``roofline``: the dominant stage kernel's algorithmic bytes per launch (9 fields x 8 B:
   stage 1 reads U and writes U*, 144 B/cell; stage 2 reads U* and U and writes U, 216 B/cell;
   360 B per zone-update) over its average event-timed duration, against the measured HBM copy
@@ -24,7 +29,8 @@ zone-updates/s (interior cells x steps / device seconds).
   workloads (rank 0). ``strips``: the 4096^2 grid split into 2 y strips on this GPU (strips.py)
   against the same grid as one solver.
 
-``--impl reference`` times that reference CPU solver alone as the reference arm.
+``--impl reference`` times that reference CPU solver alone as the reference arm; it builds the
+state in numpy and loads only the reference library (oracle/_ref), not this backend.
 Multi-GPU: the measured operator runs replicas; each rank runs the same workload on its own GPU
 and the value is the sum over ranks divided by the slowest rank's time.
 """
@@ -82,16 +88,24 @@ def parse():
                     help="requests of the served stream (0 skips it)")
     ap.add_argument("--serve-side", default="128,1024")
     ap.add_argument("--serve-tend", default="0.01,0.05")
+    ap.add_argument("--serve-rate", type=float, default=50.0,
+                    help="Poisson arrival rate of the served stream (requests/s)")
+    ap.add_argument("--serve-plain-sample", type=int, default=0,
+                    help="time the one-at-a-time FP64 path on this many seeded requests of the "
+                         "stream and estimate the whole stream from them (0: run it all)")
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="steps of the FP32-mixed vs FP64 L1 check at the headline size (0 skips)")
     return ap.parse_args()
 
 
 def initial_state(n: int) -> np.ndarray:
+    """The ghosted n^2 periodic Fourier state in the reference's StateField layout: conservative
+    interior, periodic ghosts (numpy's wrap padding is the reference's x-then-y periodic fill).
+    Pure numpy, so the reference arm builds it without loading the CUDA library."""
     from mhd_gpu_solver_b200 import workloads as wl
-    from mhd_gpu_solver_b200.mhd_solver import apply_boundary_conditions
 
-    U = wl.embed(wl.to_conservative(wl.fourier_state(n, n, SEED), GAMMA))
-    apply_boundary_conditions(U, n, n, 2, 0, 0)
-    return U
+    cons = wl.to_conservative(wl.fourier_state(n, n, SEED), GAMMA)
+    return np.pad(cons, ((0, 0), (2, 2), (2, 2)), mode="wrap")
 
 
 class ClockSampler:
@@ -262,8 +276,86 @@ def e2e_form(dev, params, host: np.ndarray, calls: int, n: int) -> dict:
         total += start.elapsed_time(end)
     nbytes = int(host.nbytes)
     return {"value": float(n) * n * E2E_STEPS * calls / (total * 1e-3), "unit": "zone-updates/s",
-            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-            "steps_per_call": E2E_STEPS, "calls": calls}
+            "h2d_bytes_per_step": nbytes / E2E_STEPS, "d2h_bytes_per_step": nbytes / E2E_STEPS,
+            "bytes_per_call": nbytes, "steps_per_call": E2E_STEPS, "calls": calls}
+
+
+def e2e_dropin(n: int, calls: int, steps_per_call: int = E2E_STEPS) -> dict:
+    """The same metric through the reference's own drop-in route: its Python module
+    (python/mhd_pybind.cpp compiled with this backend in its CUDA seam, oracle/_ref) with
+    MHDSolver.set_backend("cuda", "fp32") and MHDSolver.run(dt), which per call configures,
+    uploads the host StateField, solves to the time and downloads (include/mhd/solver_api.hpp:
+    294-321). The module offers minmod and MC only, so MC. The call is synchronous (it returns
+    after the download), so it is timed by the host clock between device synchronisations."""
+    import glob
+    import importlib
+
+    import torch
+
+    from mhd_gpu_solver_b200 import workloads as wl
+
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not glob.glob(os.path.join(ref_dir, "mhd_solver*.so")):
+        return {"unavailable": "reference module with this backend not built (oracle/_ref)"}
+    sys.path.insert(0, ref_dir)
+    try:
+        ms = importlib.import_module("mhd_solver")
+    finally:
+        sys.path.remove(ref_dir)
+    prim = wl.fourier_state(n, n, SEED)
+    s = ms.MHDSolver(n, n)
+    s.set_periodic_bc()
+    s.set_gamma(GAMMA)
+    s.set_cfl(0.4)
+    s.set_glm_alpha(0.1)
+    s.set_limiter_mc()
+    s.set_primitives(prim["rho"], prim["vx"], prim["vy"], prim["vz"], prim["p"], prim["bx"],
+                     prim["by"], prim["bz"], prim["psi"])
+    s.set_backend("cuda", "fp32")
+    r0 = s.run(1e-6)  # warm-up: device object, kernel attributes
+    # about steps_per_call steps per run() at the CFL step of the current signal speed
+    t_call = steps_per_call * 0.4 / (r0.c_h * n + r0.c_h * n)
+    s.run(t_call)  # warm-up at full length: graph capture
+    total, steps = 0.0, 0
+    for _ in range(calls):
+        k0 = s.steps
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run(t_call)
+        torch.cuda.synchronize()
+        total += time.perf_counter() - t0
+        steps += s.steps - k0
+    nbytes = 9 * (n + 4) * (n + 4) * 8
+    return {"value": float(n) * n * steps / total, "unit": "zone-updates/s",
+            "route": "reference mhd_solver module, MHDSolver.run, backend cuda/fp32, MC",
+            "steps_per_call": steps / calls, "calls": calls,
+            "h2d_bytes_per_step": nbytes * calls / steps, "d2h_bytes_per_step": nbytes * calls / steps,
+            "device": s.backend_device()}
+
+
+def accuracy_leg(host: np.ndarray, n: int, params, steps: int = 500) -> dict:
+    """The FP32-mixed result against the FP64 result after `steps` steps of the same n^2 state
+    (the headline workload), per component (mhd_gpu_solver_b200.accuracy.component_l1)."""
+    from mhd_gpu_solver_b200 import _capi
+    from mhd_gpu_solver_b200.accuracy import COMPONENTS, component_l1
+
+    outs = {}
+    for name, prec in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32)):
+        dev = _capi.DeviceSolver(n, n, precision=prec)
+        try:
+            dev.configure(_capi.BC_PERIODIC, _capi.BC_PERIODIC)
+            dev.upload(host)
+            r = dev.solve_steps(params, steps)
+            outs[name] = (dev.download(), r)
+        finally:
+            dev.close()
+    (u64, r64), (u32, r32) = outs["fp64"], outs["fp32_mixed"]
+    err = component_l1(u32, u64, r64.c_h)
+    return {"steps": steps, "same_step_count": r64.steps == r32.steps == steps,
+            "t_rel_diff": abs(r32.t - r64.t) / r64.t, "max": float(np.max(err)),
+            "per_component": {c: float(e) for c, e in zip(COMPONENTS, err)},
+            "rule": "relative L1 per component (absolute where FP64 is identically zero), "
+                    "psi on max(sum|psi|, c_h sum|B|)"}
 
 
 def bench_batched(nsolves: int, steps: int, seed: int = 1) -> dict:
@@ -452,18 +544,49 @@ def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
     return out
 
 
-def bench_served(nreq: int, side, tend) -> dict:
+def bench_served(nreq: int, side, tend, rate: float, plain_sample: int = 0) -> dict:
+    """The served stream: seeded Poisson arrivals at `rate`, FP32-mixed continuous batching
+    under the 150 GB cap, against the plain FP64 path one request at a time. With plain_sample >
+    0 the plain path runs a seeded random subsample of that many requests and its time for the
+    whole stream is estimated by a least-squares fit of per-request seconds = a + b x
+    zone-updates over the sample, summed over every request (the plain path's requests run back
+    to back at a saturating rate, so its makespan is that sum)."""
     from mhd_gpu_solver_b200.serve import make_stream, prepare, serve, serve_one_at_a_time
 
-    stream = make_stream(nreq, rate=1e4, seed=2, side=side, t_end=tend, nonideal_frac=0.3)
+    stream = make_stream(nreq, rate=rate, seed=2, side=side, t_end=tend, nonideal_frac=0.3)
     prepare(stream)  # batch autotuning of the stream's size classes, outside the timed run
-    served = serve(stream).summary()
-    plain = serve_one_at_a_time(stream).summary()
-    return {"workload": f"{nreq} requests, Poisson arrivals at 1e4/s (saturating), side "
-                        f"log-uniform in [{side[0]},{side[1]}], t_end ~ U[{tend[0]},{tend[1]}], "
-                        "Fourier or four-quadrant 50/50, 30% non-ideal, FP32-mixed, 150 GB cap",
-            "served": served, "one_at_a_time_fp64": plain,
-            "solves_per_s_ratio": served["solves_per_s"] / plain["solves_per_s"]}
+    stats = serve(stream)
+    served = stats.summary()
+    work = {c.rid: c.cells * c.steps for c in stats.completions}
+    out = {"workload": f"{nreq} requests, Poisson arrivals at {rate:g}/s, side "
+                       f"log-uniform in [{side[0]},{side[1]}], t_end ~ U[{tend[0]},{tend[1]}], "
+                       "Fourier or four-quadrant 50/50, 30% non-ideal, FP32-mixed, 150 GB cap",
+           "served": served}
+    if plain_sample <= 0 or plain_sample >= nreq:
+        plain = serve_one_at_a_time(stream).summary()
+        out["one_at_a_time_fp64"] = plain
+        out["solves_per_s_ratio"] = served["solves_per_s"] / plain["solves_per_s"]
+        return out
+    rng = np.random.Generator(np.random.PCG64(11))
+    pick = sorted(rng.choice(nreq, size=plain_sample, replace=False).tolist())
+    sample = [stream[i] for i in pick]
+    for r in sample:
+        r.arrival = 0.0  # back to back: the plain path is the bottleneck at a saturating rate
+    ps = serve_one_at_a_time(sample)
+    secs = np.array([c.finished - c.admitted for c in ps.completions])
+    zu = np.array([float(work[c.rid]) for c in ps.completions])
+    A = np.stack([np.ones_like(zu), zu], axis=1)
+    (a, b), *_ = np.linalg.lstsq(A, secs, rcond=None)
+    est = float(sum(a + b * w for w in work.values()))
+    out["one_at_a_time_fp64"] = {
+        "method": f"{plain_sample} seeded random requests of the stream run back to back; "
+                  "per-request seconds fitted as a + b x zone-updates (least squares) and summed "
+                  "over all requests",
+        "sample_requests": plain_sample, "sample_seconds": float(secs.sum()),
+        "sample_zone_updates": float(zu.sum()), "fit_a_s": float(a), "fit_b_s": float(b),
+        "estimated_makespan_s": est, "solves_per_s": nreq / est}
+    out["solves_per_s_ratio"] = served["solves_per_s"] / (nreq / est)
+    return out
 
 
 def cpu_reference_rate(U: np.ndarray, n: int, steps: int) -> dict:
@@ -554,6 +677,7 @@ def main():
     host = torch.empty(U.shape, dtype=torch.float64, pin_memory=True).numpy()
     host[...] = U
     params = _capi.make_params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=_capi.VANLEER)
+    params_mc = _capi.make_params(cfl=0.4, gamma=GAMMA, glm_alpha=0.1, limiter=_capi.MC)
 
     results = {}
     # the headline form first, on a GPU that has not yet run the FP64 form
@@ -587,6 +711,15 @@ def main():
             r["e2e"] = e2e_form(dev, params, host, args.e2e_calls, n)
         dev.close()
         results[name] = r
+    if "fp64" in results and "fp64" in args.forms.split(","):
+        # like-for-like with the reference CPU solver: FP64, MC, the same state
+        dev = _capi.DeviceSolver(n, n, precision=_capi.FP64)
+        dev.configure(_capi.BC_PERIODIC, _capi.BC_PERIODIC)
+        dev.upload(host)
+        r = time_form(dev, params_mc, args.steps, args.warmup, n)
+        r["ms_max"] = max_over_ranks(r["ms"], dist)
+        dev.close()
+        results["fp64_mc"] = r
     if "fp32_mixed" not in results or "fp64" not in results:
         if rank == 0:  # profiling run: no JSON line
             print(json.dumps({k: {kk: vv for kk, vv in v.items() if kk != "prof"}
@@ -619,6 +752,13 @@ def main():
                  "stage1_avg_ms": results["fp64"]["stage1_avg_ms"],
                  "stage2_avg_ms": results["fp64"]["stage2_avg_ms"],
                  "stage2_gbs": results["fp64"]["stage2_gbs"]},
+        "fp64_mc": {"value": replicas_value(float(n) * n * args.steps,
+                                            results["fp64_mc"]["ms_max"], world),
+                    "ms_per_step": results["fp64_mc"]["ms_max"] / args.steps,
+                    "stage1_avg_ms": results["fp64_mc"]["stage1_avg_ms"],
+                    "stage2_avg_ms": results["fp64_mc"]["stage2_avg_ms"],
+                    "note": "FP64, MC limiter, same state: the like-for-like pair of the "
+                            "reference CPU solver (cpu_baseline, the reference arm)"},
         "speedup_fp32_mixed_over_fp64": results["fp64"]["ms_max"] / ms,
         "roofline": {"bound": "hbm", "kernel": f"stage{dom} (fp32_mixed)", "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
@@ -633,6 +773,10 @@ def main():
         "e2e": mixed.get("e2e"),
         "gpu_launches": mixed["launches"],
     }
+    if rank == 0 and args.accuracy_steps > 0:
+        line["l1_fp32_mixed_vs_fp64"] = accuracy_leg(host, n, params, args.accuracy_steps)
+    if rank == 0 and args.e2e_calls > 0:
+        line["e2e_dropin"] = e2e_dropin(n, args.e2e_calls)
     if rank == 0 and args.batch_solves > 0:
         line["batched"] = bench_batched(args.batch_solves, args.batch_steps)
     if rank == 0 and args.masked_steps > 0:
@@ -642,7 +786,8 @@ def main():
     if rank == 0 and args.serve_requests > 0:
         side = tuple(int(v) for v in args.serve_side.split(","))
         tend = tuple(float(v) for v in args.serve_tend.split(","))
-        line["served"] = bench_served(args.serve_requests, side, tend)
+        line["served"] = bench_served(args.serve_requests, side, tend, args.serve_rate,
+                                      args.serve_plain_sample)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference_rate(U, n, args.cpu_steps)

@@ -183,6 +183,16 @@ int mhdb_tile_config_kind(int precision, int config);
    0), smaller masked FP64 solves configuration 0. */
 int mhdb_set_tile_config(mhdb_solver* h, int config);
 
+/* Additive, for tests of the error path: every bulk-copy wait of the TMA strip marches is bounded
+   (0.5 s); when one runs out the kernel records it in the Ctrl block, lets its copies in flight
+   land and stops, and the solve returns MHDB_CUDA_ERROR ("a bulk-copy wait exceeded its limit")
+   with the device context intact. With extra_bytes > 0 (at most 4096) the strip marches of this
+   handle arm the first row copy of the strip at the grid's origin for extra_bytes transaction
+   bytes more than its boxes deliver, so that wait runs out; the copies themselves are unchanged.
+   0 (the default) turns it off. Solves on other kernels are unaffected. No reference
+   counterpart (the reference has no bulk copies). */
+int mhdb_debug_stall_copies(mhdb_solver* h, int extra_bytes);
+
 /* ---------------------------------------------------------------- strips of one grid (additive)
 
    One grid split into y strips, one solver per strip (on one GPU or on several): each strip's
@@ -276,8 +286,13 @@ int mhdb_batch_config_info(int precision, int config, int* tile_x, int* tile_y, 
 int mhdb_batch_set_config(mhdb_batch* b, int id, int config);
 
 /* t, steps, c_h and whether the solve has finished; MHDB_MAX_STEPS / MHDB_BAD_TIMESTEP as
-   mhdb_solve would report them. */
+   mhdb_solve would report them, and MHDB_CUDA_ERROR when one of the solve's bulk-copy waits ran
+   out (the solve stopped; the other solves of the batch are unaffected). */
 int mhdb_batch_status(mhdb_batch* b, int id, mhdb_result* result, int* finished);
+
+/* Test hook of the bounded bulk-copy waits for one solve of a batch, as mhdb_debug_stall_copies
+   (TMA strip-march batch configurations only). */
+int mhdb_batch_debug_stall_copies(mhdb_batch* b, int id, int extra_bytes);
 int mhdb_batch_download(mhdb_batch* b, int id, double* const comps[9], size_t n_tot);
 int mhdb_batch_info(const mhdb_batch* b, size_t* bytes_in_use, int* live, long long* launches);
 void* mhdb_batch_stream(mhdb_batch* b);
@@ -290,20 +305,23 @@ void* mhdb_batch_stream(mhdb_batch* b);
    the stage state U* and the step control live in one file-scope device array of 16 MiB + 256 B
    that every GPU loading this library holds until the process exits.
    - u_in, u_out: device pointers to 9 dense planes of nx * ny doubles (rho, mx, my, mz, E, bx,
-     by, bz, psi; interior cells only, row-major, no ghosts); u_out may equal u_in. The caller
+     by, bz, psi; interior cells only, row-major, no ghosts); u_out must equal u_in or not
+     overlap it at all (a partial overlap is rejected with MHDB_INVALID_ARGUMENT). The caller
      passes both; the state is read from u_in and the result written to u_out.
    - Limit: nx * ny <= 233016 interior cells (16 MiB / 72 B); larger grids are rejected with
      MHDB_INVALID_ARGUMENT and a message from mhdb_last_error(NULL). No mask; boundaries
      periodic or outflow; ideal or non-ideal terms, any limiter.
-   - Work runs on `stream` (a cudaStream_t, NULL for the legacy default stream); the call returns
-     after the stream has finished the solve and result holds t, steps and c_h.
+   - Work runs on `stream` (a cudaStream_t, NULL for the legacy default stream). Each call copies
+     the step control between host and device through pageable host memory and synchronises
+     `stream` before it returns; result then holds t, steps and c_h.
    - The first call on each device looks up the device address of the scratch array
-     (cudaGetSymbolAddress) with that device current; make that first call before any stream
-     capture.
+     (cudaGetSymbolAddress) with that device current and keeps it for the life of the process
+     (a cudaDeviceReset of that device would leave it stale); make that first call before any
+     stream capture.
    - Every call shares the one scratch array, which keeps the last call's contents: the step
      control is reset at the start of each call and U* is fully rewritten before it is read.
-     Calls whose work overlaps on the GPU (several streams, threads or processes sharing the
-     library on one device) race on that array. */
+     Calls in one process whose work overlaps on the GPU (several streams or threads on the same
+     device) race on that array; each process has its own copy. */
 int mhdb_solve_steps_noalloc_f64(const mhdb_grid* grid, int bc_x, int bc_y,
                                  const mhdb_params* params, int nsteps, const double* u_in,
                                  double* u_out, mhdb_result* result, void* stream);

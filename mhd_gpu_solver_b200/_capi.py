@@ -33,6 +33,7 @@ EXPORTS = (
     "mhdb_batch_launch", "mhdb_batch_poll", "mhdb_batch_config_count", "mhdb_batch_config_info",
     "mhdb_batch_set_config", "mhdb_set_cell_size", "mhdb_set_reduce_rows", "mhdb_strip_view", "mhdb_strip_begin",
     "mhdb_strip_step", "mhdb_strip_finish", "mhdb_strip_poll", "mhdb_strip_end",
+    "mhdb_debug_stall_copies", "mhdb_batch_debug_stall_copies",
 )
 
 
@@ -113,6 +114,7 @@ def _load() -> C.CDLL:
                                    C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "mhdb_tile_config_kind": ([C.c_int, C.c_int], C.c_int),
         "mhdb_set_tile_config": ([h, C.c_int], C.c_int),
+        "mhdb_debug_stall_copies": ([h, C.c_int], C.c_int),
         "mhdb_solve_steps_noalloc_f64": ([C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(Params),
                                           C.c_int, C.c_void_p, C.c_void_p, C.POINTER(Result),
                                           C.c_void_p], C.c_int),
@@ -131,6 +133,7 @@ def _load() -> C.CDLL:
         "mhdb_batch_config_info": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_set_config": ([b, C.c_int, C.c_int], C.c_int),
+        "mhdb_batch_debug_stall_copies": ([b, C.c_int, C.c_int], C.c_int),
         "mhdb_batch_poll": ([b, C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_status": ([b, C.c_int, C.POINTER(Result), C.POINTER(C.c_int)], C.c_int),
         "mhdb_batch_download": ([b, C.c_int, _PPD, C.c_size_t], C.c_int),
@@ -295,6 +298,11 @@ class DeviceSolver:
 
     def set_tile_config(self, config: int) -> None:
         raise_for(lib.mhdb_set_tile_config(self._h, int(config)), self._h)
+
+    def debug_stall_copies(self, extra_bytes: int) -> None:
+        """Test hook: make one bulk-copy wait of the TMA strip marches run out
+        (mhdb_debug_stall_copies); 0 turns it off."""
+        raise_for(lib.mhdb_debug_stall_copies(self._h, int(extra_bytes)), self._h)
 
     # Deferred solves of one strip of a split grid (strips.py drives them).
     def set_cell_size(self, dx: float, dy: float) -> None:

@@ -102,6 +102,11 @@ class BatchSolver:
         """Run this solve with batch configuration `config` (-1: chosen by its size)."""
         self._raise(_capi.lib.mhdb_batch_set_config(self._b, int(sid), int(config)))
 
+    def debug_stall_copies(self, sid: int, extra_bytes: int) -> None:
+        """Test hook: make one bulk-copy wait of this solve's TMA strip march run out
+        (mhdb_batch_debug_stall_copies); 0 turns it off."""
+        self._raise(_capi.lib.mhdb_batch_debug_stall_copies(self._b, int(sid), int(extra_bytes)))
+
     def remove(self, sid: int) -> None:
         self._raise(_capi.lib.mhdb_batch_remove(self._b, int(sid)))
         self._shapes.pop(sid, None)

@@ -842,7 +842,7 @@ void add_solve(mhdb_batch* b, const mhdb_grid* grid, const mhdb_params* params, 
     check(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
     s.last = b->ctrl_host[slot];
     s.live = true;
-    if (s.last.status & kStatusBadDt) {
+    if (s.last.status & (kStatusBadDt | kStatusWaitTimeout)) {
         s.last.finished = 1;
     }
     int sid;
@@ -975,6 +975,23 @@ int mhdb_batch_set_config(mhdb_batch* b, int id, int config)
     });
 }
 
+int mhdb_batch_debug_stall_copies(mhdb_batch* b, int id, int extra_bytes)
+{
+    return guarded(b, [&] {
+        if (id < 0 || id >= static_cast<int>(b->solves.size()) || !b->solves[id].live) {
+            throw BatchFail{MHDB_INVALID_ARGUMENT, "unknown solve id"};
+        }
+        if (extra_bytes < 0 || extra_bytes > 4096) {
+            throw BatchFail{MHDB_INVALID_ARGUMENT, "stall bytes must lie in [0, 4096]"};
+        }
+        SolveRec& s = b->solves[id];
+        if (s.k.stall_tx != extra_bytes) {
+            s.k.stall_tx = extra_bytes;
+            b->dirty = true; // the descriptors carry the constants
+        }
+    });
+}
+
 int mhdb_batch_launch(mhdb_batch* b, int nsteps)
 {
     return guarded(b, [&] {
@@ -1017,6 +1034,9 @@ int mhdb_batch_status(mhdb_batch* b, int id, mhdb_result* result, int* finished)
         }
         if (finished != nullptr) {
             *finished = s.last.finished;
+        }
+        if (s.last.status & kStatusWaitTimeout) {
+            throw BatchFail{MHDB_CUDA_ERROR, "stage kernel: a bulk-copy wait exceeded its limit"};
         }
         if (s.last.status & kStatusBadDt) {
             throw BatchFail{MHDB_BAD_TIMESTEP, "ssp_rk2_step requires positive dt"};

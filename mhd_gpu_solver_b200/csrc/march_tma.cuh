@@ -124,13 +124,16 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
     }
     __syncwarp();
 
+    // Consts::stall_tx (timeout tests only): extra transaction bytes on the first halo copy of
+    // the strip at the origin, which no copy delivers; every copy itself stays well-formed.
+    const uint32_t stall = (x0 == 0 && y0 == 0) ? static_cast<uint32_t>(k.stall_tx) : 0u;
     // Item i of the halo stream is row y0 + 2 + i; item i of the own stream is row y0 + i; both
     // use slot i & 1, whose (i >> 1)-th phase completes it.
     auto issue_halo = [&](int i) {
         const uint32_t slot = static_cast<uint32_t>(i & 1);
         const uint32_t bar = bar_s + 8 * slot;
         const int yy = map_index(y0 + 2 + i, g.ny, g.bc_y);
-        mbar_arrive_expect_tx(bar, Lay::kHaloBytes);
+        mbar_arrive_expect_tx(bar, Lay::kHaloBytes + (i == 0 ? stall : 0u));
         tma_load_3d(halo_s + slot * Lay::kHaloSlot, &m.in_halo, bar, x0 - 4, yy, 0);
         if constexpr (Lay::kHaloBoxes == 2) {
             tma_load_3d(halo_s + slot * Lay::kHaloSlot + Lay::kHaloBoxSlot, &m.delta_halo, bar,
@@ -570,7 +573,7 @@ struct BatchSolveTma {
 // Persistent TMA strip march over a block work-list of many independent solves (items: solve
 // index, block index), as batch_march_kernel; the tensor maps come from the descriptor array in
 // global memory (lane 0 acquires them before its copies). A warp whose copies timed out processes
-// no further items (the solve reports kStatusWaitTimeout).
+// no further items: the solves of the items it would have run report kStatusWaitTimeout too.
 template <int L, bool NI, int STAGE, int LY, int NW, int MINB, bool HF, int ST>
 __global__ void __launch_bounds__(NW * 32, MINB) batch_march_tma_kernel(
     const BatchSolveTma* solves, const int2* __restrict__ work, int nwork)
@@ -605,7 +608,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) batch_march_tma_kernel(
         const int x0 = ((it.y % s_tiles_x) * NW + warp) * kMarchOwned;
         const int y0 = (it.y / s_tiles_x) * LY;
         double smax = 0.0;
-        if (x0 < sa.geom.nx && !failed) { // warp-uniform
+        if (x0 < sa.geom.nx && failed) { // warp-uniform
+            // this warp's barriers are unusable after a timed-out wait, so it cannot advance the
+            // item: its solve reports the timeout instead of skipping cells
+            if (lane == 0) {
+                atomicOr(&sa.ctrl->status, static_cast<int>(kStatusWaitTimeout));
+            }
+        } else if (x0 < sa.geom.nx) { // warp-uniform
             if (lane == 0) {
                 tensormap_acquire(&m.in_halo);
                 tensormap_acquire(&m.in_own);
@@ -660,7 +669,11 @@ __global__ void __launch_bounds__(NW * 32, MINB) batch_march_delta_kernel(
         const int x0 = ((it.y % s_tiles_x) * NW + warp) * kMarchOwned;
         const int y0 = (it.y / s_tiles_x) * LY;
         double smax = 0.0;
-        if (x0 < sa.geom.nx && !failed) { // warp-uniform
+        if (x0 < sa.geom.nx && failed) { // warp-uniform: as in batch_march_tma_kernel
+            if (lane == 0) {
+                atomicOr(&sa.ctrl->status, static_cast<int>(kStatusWaitTimeout));
+            }
+        } else if (x0 < sa.geom.nx) { // warp-uniform
             if (lane == 0) {
                 tensormap_acquire(&m.in_halo);
                 if constexpr (STAGE == 2) {

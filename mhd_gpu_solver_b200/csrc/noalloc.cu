@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -58,7 +59,8 @@ int cuda_fail(cudaError_t e, const char* what)
 
 // Device address of the scratch array on the current device. In host code the array's name is
 // only a host-side stand-in, so the address is looked up once per device with that device
-// current and cached.
+// current and cached for the life of the process (a cudaDeviceReset of that device would leave
+// the cached address stale).
 cudaError_t scratch_address(int device, void** out)
 {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
@@ -182,10 +184,18 @@ int mhdb_solve_steps_noalloc_f64(const mhdb_grid* grid, int bc_x, int bc_y,
     Ctrl* ctrl = static_cast<Ctrl*>(scratch);
     double* ustar = reinterpret_cast<double*>(static_cast<unsigned char*>(scratch) + kCtrlBytes);
 
+    // u_out either is u_in or lies wholly apart from it: a partial overlap would make the copy
+    // below overlap itself and the stages read a half-written state.
+    const size_t state_bytes = 9 * cells * sizeof(double);
+    const uintptr_t in0 = reinterpret_cast<uintptr_t>(u_in);
+    const uintptr_t out0 = reinterpret_cast<uintptr_t>(u_out);
+    if (u_out != u_in && in0 < out0 + state_bytes && out0 < in0 + state_bytes) {
+        return fail(MHDB_INVALID_ARGUMENT, "u_out must equal u_in or not overlap it");
+    }
     // The stage-2 kernel updates its state in place, so the caller's output buffer carries the
     // state from the start.
     if (u_out != u_in) {
-        e = cudaMemcpyAsync(u_out, u_in, 9 * cells * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        e = cudaMemcpyAsync(u_out, u_in, state_bytes, cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) {
             return cuda_fail(e, "cudaMemcpyAsync");
         }

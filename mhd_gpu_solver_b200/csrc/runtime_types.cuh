@@ -36,6 +36,10 @@ struct Consts {
     double cfl, eta_max, dt_diff;
     NonIdealCoef ni;
     int ni_any;
+    // Test hook of the bounded bulk-copy waits (zero in every ordinary solve): the TMA strip
+    // marches arm the first row copy of the strip at the grid's origin for this many transaction
+    // bytes more than its boxes deliver, so that phase never completes and its wait runs out.
+    int stall_tx;
 };
 
 // kStatusWaitTimeout: a stage kernel gave up waiting for one of its own bulk copies (bounded

@@ -6,9 +6,10 @@
 //   * the padded fluid mask, a device Ctrl block (FP64 clock, dt, c_h, step counter),
 //   * a ghosted staging buffer for host <-> device exchange in the reference layout,
 //   * one CUDA stream and cached CUDA graphs of batches of RK2 steps.
-// The time loop keeps dt on the device: each step is two launches (stage 1, stage 2 with the
-// CFL reduction fused in) and the host only polls Ctrl once per batch of steps, as the reference
-// CUDA backend does (src/cuda/cuda_solver.cu:601-655 in the reference project).
+// The time loop keeps dt and the clock on the device: each step is two launches (stage 1, stage 2
+// with the CFL reduction fused in), replayed as captured graphs of kGraphBatch steps, and a
+// time-based solve reads the Ctrl block back only after each queue of the steps that its current
+// dt says remain (steps_to_queue); the device ends the solve.
 
 #include "mhd_b200.h"
 
@@ -246,6 +247,7 @@ struct mhdb_solver {
     int graph_next = 0; // entry to replace next
 
     int tile_config = -1; // index into the compiled tile configurations (-1: by grid size)
+    int stall_tx = 0;     // test hook of the bounded copy waits (mhdb_debug_stall_copies)
     bool profiling = false;
     std::vector<Prof> prof_pending;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pool;
@@ -326,6 +328,7 @@ Consts make_consts(const mhdb_solver* h, const mhdb_params* p)
     k.ni.eta_ambipolar = p->eta_ambipolar;
     k.ni_any = (p->ohmic && p->eta_ohm != 0.0) || (p->hall && p->eta_hall != 0.0) ||
                (p->ambipolar && p->eta_ambipolar != 0.0);
+    k.stall_tx = h->stall_tx;
     return k;
 }
 
@@ -555,7 +558,8 @@ std::vector<double> plan_key(const mhdb_solver* h, const mhdb_params* p, const S
             static_cast<double>(h->grid.nx), static_cast<double>(h->grid.ny),
             static_cast<double>(h->tile_config),
             h->grid.x_min, h->grid.x_max, h->grid.y_min, h->grid.y_max, h->dx, h->dy,
-            static_cast<double>(h->geom.ry0), static_cast<double>(h->geom.ry1)};
+            static_cast<double>(h->geom.ry0), static_cast<double>(h->geom.ry1),
+            static_cast<double>(h->stall_tx)};
 }
 
 void launch_steps(mhdb_solver* h, const mhdb_params* p, const StepPlan& s, int n)
@@ -647,6 +651,27 @@ void read_ctrl(mhdb_solver* h)
     MHDB_CHECK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost,
                                h->stream));
     MHDB_CHECK(cudaStreamSynchronize(h->stream));
+}
+
+// Steps to queue before the next read of the Ctrl block in a time-based solve. The device
+// decides where the solve ends (finish_step sets `finished`, and steps queued past that point
+// return at once), so the host only sizes the queue: the steps that the dt of the step about to
+// run says remain, ceil((t_end - t) / dt), capped by the steps max_steps leaves, and rounded up
+// to whole captured graph batches once a batch fits (at most kGraphBatch - 1 queued steps then
+// do nothing). A dt that shrinks as the flow steepens costs one more round.
+int steps_to_queue(const Ctrl& c)
+{
+    const int left = std::max(1, c.max_steps - c.steps);
+    const double need = std::ceil((c.t_end - c.t) / c.dt);
+    if (!(need > 0.0) || need >= static_cast<double>(left)) {
+        return left;
+    }
+    int n = static_cast<int>(need);
+    if (n >= kGraphBatch) {
+        n = static_cast<int>(std::min<long long>(
+            left, (static_cast<long long>(n) + kGraphBatch - 1) / kGraphBatch * kGraphBatch));
+    }
+    return n;
 }
 
 void ensure_staging(mhdb_solver* h)
@@ -770,28 +795,10 @@ int run_solve(mhdb_solver* h, const mhdb_params* p, int fixed_steps, mhdb_result
             read_ctrl(h);
         } else {
             start_solve(h, s, p->t_end, p->max_steps);
-            // Batches of steps between host polls, sized from the observed dt
-            // (same policy as the reference CUDA backend: 4 first, then an estimate, <= 256).
-            int batch = 4;
-            double last_t = 0.0;
-            int last_steps = 0;
             read_ctrl(h);
             while (h->ctrl_host->finished == 0) {
-                batch = std::min(batch, std::max(1, p->max_steps - h->ctrl_host->steps));
-                launch_steps(h, p, s, batch);
+                launch_steps(h, p, s, steps_to_queue(*h->ctrl_host));
                 read_ctrl(h);
-                const Ctrl& c = *h->ctrl_host;
-                if (c.finished != 0) {
-                    break;
-                }
-                const double dt_avg = c.steps > last_steps ? (c.t - last_t) / (c.steps - last_steps) : 0.0;
-                last_t = c.t;
-                last_steps = c.steps;
-                int est = batch * 2;
-                if (dt_avg > 0.0) {
-                    est = static_cast<int>(std::ceil((p->t_end - c.t) / dt_avg)) + 1;
-                }
-                batch = std::clamp(est, 1, 256);
             }
         }
         settle_buffers(h, s);
@@ -1186,6 +1193,19 @@ int mhdb_set_tile_config(mhdb_solver* h, int config)
         return MHDB_INVALID_ARGUMENT;
     }
     h->tile_config = config;
+    return MHDB_OK;
+}
+
+int mhdb_debug_stall_copies(mhdb_solver* h, int extra_bytes)
+{
+    if (h == nullptr) {
+        return MHDB_INVALID_ARGUMENT;
+    }
+    if (extra_bytes < 0 || extra_bytes > 4096) {
+        h->last_error = "stall bytes must lie in [0, 4096]";
+        return MHDB_INVALID_ARGUMENT;
+    }
+    h->stall_tx = extra_bytes;
     return MHDB_OK;
 }
 

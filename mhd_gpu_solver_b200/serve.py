@@ -127,6 +127,8 @@ class ServeStats:
     peak_bytes: int = 0
     max_active: int = 0
     chunks: int = 0
+    joins: int = 0      # requests admitted while others were on the GPU (continuous batching)
+    cap_waits: int = 0  # admission rounds in which the next request waited for memory
     states: dict = field(default_factory=dict)  # rid -> final state when kept
 
     def summary(self) -> dict:
@@ -138,7 +140,8 @@ class ServeStats:
                 "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "peak_hbm_bytes": self.peak_bytes, "max_active": self.max_active,
-                "chunks": self.chunks}
+                "chunks": self.chunks, "joined_mid_flight": self.joins,
+                "admission_waits_for_memory": self.cap_waits}
 
 
 def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
@@ -179,8 +182,11 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
                 req = queue[0]
                 need = state_bytes(req.n, req.n)
                 if in_use + need > memory_cap and (active or done):
+                    stats.cap_waits += 1
                     break
                 queue.popleft()
+                if active:
+                    stats.joins += 1
                 sid = batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
                 in_use += need
                 active[sid] = (req, time.perf_counter() - start)

@@ -371,18 +371,16 @@ class StripSolver:
             for _ in range(nsteps):
                 self._step()
         else:
-            # batches of steps between polls: 4 first, then an estimate from the observed dt,
-            # at most 256 (the policy of the single-grid solve)
-            batch, last_t, last_n = 4, 0.0, 0
+            # Rounds of steps between polls: one step first (to measure dt), then the steps that
+            # remain at the mean dt of the steps taken so far. The strips' common clock ends the
+            # solve on the device (steps issued past the end do nothing), and a dt that shrinks
+            # as the flow steepens costs one more round.
             while True:
                 done, n, t = self._poll()
                 if done:
                     break
-                if n > last_n:
-                    dt = (t - last_t) / (n - last_n)
-                    batch = min(256, max(1, math.ceil((params.t_end - t) / dt) + 1))
-                last_t, last_n = t, n
-                for _ in range(max(1, min(batch, params.max_steps - n))):
+                queue = 1 if n == 0 or t <= 0.0 else math.ceil((params.t_end - t) * n / t)
+                for _ in range(max(1, min(queue, params.max_steps - n))):
                     self._step()
         results = [e.end() for e in self.engines]
         return results[0]

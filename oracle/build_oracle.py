@@ -2,9 +2,10 @@
 
 * ``oracle/libmhd_oracle.so``: the C restatement (``mhd_oracle.c``), built with gcc for
   baseline x86-64 (no FMA contraction is possible there, so every operation rounds once,
-  in program order).
+  in program order) and OpenMP (its loops over cells and rows run on all host threads; the
+  results do not depend on the thread count).
 * ``oracle/_ref/libmhd_ref_<isa>.so``: the reference CPU solver compiled from its own
-  headers where they lie (``REFERENCE_ROOT/include``), wrapped by ``ref_driver.cpp``, with
+  headers where they lie (``$MHD_REFERENCE_ROOT/include``), wrapped by ``ref_driver.cpp``, with
   the reference's release flags (``-O3 -ffp-contract=fast -fno-math-errno
   -fno-trapping-math``; cmake/MHDCompilerFlags.cmake:29-35) for two ISA levels
   (x86-64-v4 = AVX-512F, x86-64-v3 = AVX2+FMA). Built only where the reference checkout
@@ -24,7 +25,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = os.environ.get("MHD_REFERENCE_ROOT", "/root/reference")
+
+
+def reference_root() -> str | None:
+    """The reference checkout named by MHD_REFERENCE_ROOT (unset: no reference build)."""
+    return os.environ.get("MHD_REFERENCE_ROOT") or None
 
 ORACLE_SO = os.path.join(HERE, "libmhd_oracle.so")
 REF_ISAS = {"avx512": "x86-64-v4", "avx2": "x86-64-v3"}
@@ -47,13 +52,14 @@ def build_oracle(force: bool = False) -> str:
     src = os.path.join(HERE, "mhd_oracle.c")
     hdr = os.path.join(HERE, "mhd_oracle.h")
     if force or _stale(ORACLE_SO, [src, hdr]):
-        _run(["gcc", "-std=c99", "-O2", "-fPIC", "-shared", "-ffp-contract=off",
+        _run(["gcc", "-std=c99", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
               "-march=x86-64", "-Wall", "-Wextra", src, "-o", ORACLE_SO, "-lm"])
     return ORACLE_SO
 
 
 def reference_available() -> bool:
-    return os.path.isdir(os.path.join(REFERENCE_ROOT, "include", "mhd"))
+    root = reference_root()
+    return root is not None and os.path.isdir(os.path.join(root, "include", "mhd"))
 
 
 def build_ref(force: bool = False) -> list[str]:
@@ -63,7 +69,7 @@ def build_ref(force: bool = False) -> list[str]:
     os.makedirs(REF_DIR, exist_ok=True)
     src = os.path.join(HERE, "ref_driver.cpp")
     hdr = os.path.join(HERE, "mhd_oracle.h")
-    inc = os.path.join(REFERENCE_ROOT, "include")
+    inc = os.path.join(reference_root(), "include")
     ref_headers = []
     for root, _dirs, files in os.walk(inc):
         ref_headers += [os.path.join(root, f) for f in files if f.endswith(".hpp")]
@@ -113,7 +119,7 @@ def build_ref_with_b200(force: bool = False) -> list[str]:
     import pybind11
 
     os.makedirs(REF_DIR, exist_ok=True)
-    inc = os.path.join(REFERENCE_ROOT, "include")
+    inc = os.path.join(reference_root(), "include")
     gen = _build_info_header()
     common = ["g++", "-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-fno-trapping-math",
               "-ffp-contract=fast", "-march=x86-64-v3", "-pthread", "-DMHD_HAS_CUDA=1",
@@ -121,13 +127,13 @@ def build_ref_with_b200(force: bool = False) -> list[str]:
     link = ["-L", PKG_DIR, "-l:libmhd_b200.so", "-Wl,-rpath,$ORIGIN/../../mhd_gpu_solver_b200"]
     outs = []
     mod = os.path.join(REF_DIR, "mhd_solver" + sysconfig.get_config_var("EXT_SUFFIX"))
-    src_mod = os.path.join(REFERENCE_ROOT, "python", "mhd_pybind.cpp")
+    src_mod = os.path.join(reference_root(), "python", "mhd_pybind.cpp")
     if force or _stale(mod, [src_mod, ADAPTER, lib]):
         _run(common + ["-fPIC", "-shared", "-I", pybind11.get_include(),
                        "-I", sysconfig.get_paths()["include"], src_mod, ADAPTER, "-o", mod] + link)
     outs.append(mod)
     gate = os.path.join(REF_DIR, "mhd_backend_compare")
-    src_gate = os.path.join(REFERENCE_ROOT, "tools", "mhd_backend_compare.cpp")
+    src_gate = os.path.join(reference_root(), "tools", "mhd_backend_compare.cpp")
     if force or _stale(gate, [src_gate, ADAPTER, lib]):
         _run(common + [src_gate, ADAPTER, "-o", gate] + link)
     outs.append(gate)
@@ -142,12 +148,12 @@ def build_cuda_bench(force: bool = False) -> list[str]:
     if not reference_available() or not os.path.exists(lib) or not os.path.exists(nvcc):
         return []
     os.makedirs(REF_DIR, exist_ok=True)
-    inc = os.path.join(REFERENCE_ROOT, "include")
+    inc = os.path.join(reference_root(), "include")
     drv = os.path.join(HERE, "cuda_backend_bench.cpp")
     host = ["g++", "-std=c++20", "-O3", "-DNDEBUG", "-fno-math-errno", "-fno-trapping-math",
             "-ffp-contract=fast", "-march=x86-64-v3", "-pthread", "-DMHD_HAS_CUDA=1", "-I", inc]
     outs = []
-    src_cu = os.path.join(REFERENCE_ROOT, "src", "cuda", "cuda_solver.cu")
+    src_cu = os.path.join(reference_root(), "src", "cuda", "cuda_solver.cu")
     obj = os.path.join(REF_DIR, "reference_cuda_solver.o")
     ref_bin = os.path.join(REF_DIR, "cuda_bench_reference")
     if force or _stale(ref_bin, [src_cu, drv]):
@@ -164,6 +170,9 @@ def build_cuda_bench(force: bool = False) -> list[str]:
 
 
 if __name__ == "__main__":
+    if not reference_available():
+        sys.stderr.write("MHD_REFERENCE_ROOT does not name a reference checkout: building the C "
+                         "oracle only\n")
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
     print(build_ref_with_b200(force="--force" in sys.argv))

@@ -1,8 +1,11 @@
 /*
  * CPU oracle for the 2D GLM-MHD operator — TEST INFRASTRUCTURE ONLY (see mhd_oracle.h).
  *
- * Plain C99, FP64, one thread. Every function cites the reference file:line it restates
- * (paths relative to the reference project root). Face fluxes are kept in full-grid arrays
+ * Plain C99, FP64. Every function cites the reference file:line it restates (paths relative to
+ * the reference project root). Built with OpenMP, the loops over cells, rows and faces run on all
+ * host threads: every value they write depends only on inputs of the same pass, so the results do
+ * not depend on the thread count; the CFL maximum is combined per row, and the diagnostics sums
+ * run in one thread in row order. Face fluxes are kept in full-grid arrays
  * instead of the reference's three rolling rows (include/mhd/rhs.hpp:186-239); each face is
  * still evaluated once from the same four cells, so the arithmetic is the same.
  */
@@ -442,8 +445,16 @@ static void cfl_dt(const geom* G, const mhdo_params* p, const uint8_t* mask, con
 {
     const double inv_dx = 1.0 / G->dx;
     const double inv_dy = 1.0 / G->dy;
-    double c_h = 0.0;
+    /* per-row maxima (any thread may take any row), then the maximum over the rows in order */
+    double* row_max = (double*)malloc((size_t)G->ny * sizeof(double));
+    if (row_max == NULL) {
+        *dt_out = NAN; /* the solve loop rejects a dt that is not positive */
+        *ch_out = NAN;
+        return;
+    }
+    #pragma omp parallel for schedule(static)
     for (int j = G->ng; j < G->ng + G->ny; ++j) {
+        double m = 0.0;
         for (int i = G->ng; i < G->ng + G->nx; ++i) {
             if (mask != NULL && !is_fluid_global(G, mask, i, j)) {
                 continue;
@@ -452,9 +463,15 @@ static void cfl_dt(const geom* G, const mhdo_params* p, const uint8_t* mask, con
             const double s = cell_max_signal_speed(
                 U[0 * G->n + k], U[1 * G->n + k], U[2 * G->n + k], U[3 * G->n + k],
                 U[4 * G->n + k], U[5 * G->n + k], U[6 * G->n + k], U[7 * G->n + k], p->gamma);
-            c_h = vmax(c_h, s);
+            m = vmax(m, s);
         }
+        row_max[j - G->ng] = m;
     }
+    double c_h = 0.0;
+    for (int j = 0; j < G->ny; ++j) {
+        c_h = vmax(c_h, row_max[j]);
+    }
+    free(row_max);
     double dt = (c_h <= 0.0) ? HUGE_VAL : p->cfl / (c_h * inv_dx + c_h * inv_dy);
     const double eta_max = max_diffusivity(p);
     if (eta_max > 0.0) {
@@ -604,6 +621,7 @@ static void compute_rhs(const geom* G, const mhdo_params* p, const uint8_t* mask
     double* W = w->prim;
 
     /* Primitives over every cell, ghosts included (cpu_rows.hpp:129-155). */
+    #pragma omp parallel for schedule(static)
     for (size_t k = 0; k < G->n; ++k) {
         const double rho = U[0 * G->n + k], mx = U[1 * G->n + k], my = U[2 * G->n + k];
         const double mz = U[3 * G->n + k], e = U[4 * G->n + k];
@@ -629,6 +647,7 @@ static void compute_rhs(const geom* G, const mhdo_params* p, const uint8_t* mask
         const double* bx = W + 5 * G->n;
         const double* by = W + 6 * G->n;
         const double* bz = W + 7 * G->n;
+        #pragma omp parallel for schedule(static)
         for (int j = 1; j < G->nyt - 1; ++j) {
             for (int i = 1; i < G->nxt - 1; ++i) {
                 const size_t idx = (size_t)j * nx + i;
@@ -648,6 +667,7 @@ static void compute_rhs(const geom* G, const mhdo_params* p, const uint8_t* mask
     const double* J = w->J;
 
     /* x-faces i-1/2 for i = ng .. ng + nx, rows ng .. ng + ny - 1 (cpu_rows.hpp:84-113). */
+    #pragma omp parallel for schedule(static)
     for (int jj = 0; jj < G->ny; ++jj) {
         const int j = jj + G->ng;
         for (int k = 0; k <= G->nx; ++k) {
@@ -672,6 +692,7 @@ static void compute_rhs(const geom* G, const mhdo_params* p, const uint8_t* mask
         }
     }
     /* y-faces j-1/2 for j = ng .. ng + ny, columns ng .. ng + nx - 1. */
+    #pragma omp parallel for schedule(static)
     for (int jj = 0; jj <= G->ny; ++jj) {
         const int j = jj + G->ng;
         for (int k = 0; k < G->nx; ++k) {
@@ -701,6 +722,7 @@ static void compute_rhs(const geom* G, const mhdo_params* p, const uint8_t* mask
     const double inv_dy = 1.0 / G->dy;
     const double h = vmin(G->dx, G->dy);
     const double psi_damp = (c_h > 0.0 && p->glm_alpha > 0.0) ? (c_h * p->glm_alpha / h) : 0.0;
+    #pragma omp parallel for schedule(static)
     for (int jj = 0; jj < G->ny; ++jj) {
         const int j = jj + G->ng;
         for (int k = 0; k < G->nx; ++k) {
@@ -757,6 +779,7 @@ static void ssp_rk2_step(const mhdo_grid* g, const geom* G, const mhdo_params* p
         mhdo_wall_fill(g, mask, p->gamma, U);
     }
     compute_rhs(G, p, mask, c_h, U, R, w);
+    #pragma omp parallel for schedule(static)
     for (size_t k = 0; k < tot; ++k) {
         Us[k] = U[k] + dt * R[k];
     }
@@ -766,6 +789,7 @@ static void ssp_rk2_step(const mhdo_grid* g, const geom* G, const mhdo_params* p
     }
     compute_rhs(G, p, mask, c_h, Us, R, w);
     const double half_dt = 0.5 * dt;
+    #pragma omp parallel for schedule(static)
     for (size_t k = 0; k < tot; ++k) {
         U[k] = 0.5 * (U[k] + Us[k]) + half_dt * R[k];
     }

@@ -5,6 +5,7 @@ from __future__ import annotations
 import numpy as np
 
 from mhd_gpu_solver_b200 import workloads as wl
+from mhd_gpu_solver_b200.accuracy import component_l1
 from oracle import oracle as orc
 
 
@@ -32,6 +33,31 @@ def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     num = np.abs(ai - bi).reshape(9, -1).sum(axis=1)
     den = np.abs(bi).reshape(9, -1).sum(axis=1)
     return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)
+
+
+def signal_speed(U: np.ndarray, gamma: float = 5.0 / 3.0, ng: int = 2) -> float:
+    """Maximum signal speed of a state (the GLM speed c_h its next step would take)."""
+    ny, nx = U.shape[1] - 2 * ng, U.shape[2] - 2 * ng
+    return orc.cfl(U, orc.Grid(nx, ny, ng), orc.Params(gamma=gamma))[1]
+
+
+def component_errors(a: np.ndarray, b: np.ndarray, c_h: float | None = None,
+                     gamma: float = 5.0 / 3.0) -> np.ndarray:
+    """Per-component L1 error of a against b over the interior, every component held
+    (mhd_gpu_solver_b200.accuracy.component_l1: relative L1, absolute where b is identically
+    zero, psi on the scale max(sum|psi|, c_h sum|B|)). c_h defaults to the maximum signal speed
+    of b (the speed of its next step)."""
+    if c_h is None:
+        c_h = signal_speed(b, gamma)
+    return component_l1(a, b, c_h)
+
+
+def assert_components(a: np.ndarray, b: np.ndarray, tol: float, c_h: float | None = None,
+                      gamma: float = 5.0 / 3.0, what=None) -> np.ndarray:
+    """component_errors(a, b) <= tol for all nine components; returns the errors."""
+    err = component_errors(a, b, c_h, gamma)
+    assert np.all(err <= tol), (what, err)
+    return err
 
 
 def rel_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:

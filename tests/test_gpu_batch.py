@@ -12,7 +12,7 @@ from mhd_gpu_solver_b200 import workloads as wl
 from mhd_gpu_solver_b200.batch import BatchSolver, fixed_params
 from mhd_gpu_solver_b200.mhd_solver import apply_boundary_conditions
 from oracle import oracle as orc
-from tests.helpers import rel_l1
+from tests.helpers import assert_components
 
 pytestmark = pytest.mark.gpu
 
@@ -76,8 +76,7 @@ def test_fixed_step_batch_equals_single_solves(precision):
         # held to the parity tolerance of each form.
         tol = 1e-12 if precision == _capi.FP64 else 1e-6
         assert abs(r.t - rr.t) <= tol * rr.t and abs(r.c_h - rr.c_h) <= tol * rr.c_h
-        err = rel_l1(got, ref)
-        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= tol), (i, err)
+        assert_components(got, ref, tol, rr.c_h, what=i)
     b.close()
 
 
@@ -96,7 +95,7 @@ def test_time_based_batch_and_fp64_oracle():
         ref, rr = single(U, case, _capi.FP64, t_end=t_end)
         assert fin and r.steps == rr.steps and r.t == rr.t == t_end
         got = b.download(sid)
-        assert np.all(rel_l1(got, ref) <= 1e-12)
+        assert_components(got, ref, 1e-12, rr.c_h)
         nx, ny, gamma, bc, lim, ni, _ = case
         op = orc.Params(t_end=t_end, gamma=gamma, limiter=lim)
         if ni:
@@ -104,7 +103,7 @@ def test_time_based_batch_and_fp64_oracle():
             op.eta_ohm, op.eta_hall, op.eta_ambipolar = 1e-3, 1e-2, 1e-3
         oref, ot, osteps, _ = orc.solve(U, orc.Grid(nx, ny), op, bc)
         assert osteps == r.steps
-        assert np.all(rel_l1(got, oref) <= 1e-12)
+        assert_components(got, oref, 1e-12, r.c_h)
     b.close()
 
 
@@ -253,8 +252,8 @@ def test_increment_form_batch_with_odd_step_counts():
                 b.set_config(live, 0)
             b.set_config(live, 3)
         b.close()
-    for a, c in zip(outs[0], outs[3]):
-        assert np.all(rel_l1(c, a)[[0, 1, 2, 4, 5, 6]] <= 1e-6)
+    for a, c, case in zip(outs[0], outs[3], cases):
+        assert_components(c, a, 1e-6, gamma=case[2])
 
 
 def test_every_batch_configuration_gives_the_same_values():
@@ -281,15 +280,14 @@ def test_every_batch_configuration_gives_the_same_values():
         outs.append([b.download(i) for i in ids])
         b.close()
     for cfg, other in zip(configs[1:], outs[1:]):
-        for a, c in zip(outs[0], other):
-            assert np.all(rel_l1(c, a)[[0, 1, 2, 4, 5, 6]] <= 1e-6), cfg
+        for a, c, case in zip(outs[0], other, cases):
+            assert_components(c, a, 1e-6, gamma=case[2], what=cfg)
     b64 = BatchSolver(_capi.FP64)
     ids = [b64.add(U, fixed_params(20, **params_of(c)), c[3], fixed_steps=True)
            for U, c in zip(states, cases)]
     b64.step(20)
-    for sid, got in zip(ids, outs[0]):
-        err = rel_l1(got, b64.download(sid))
-        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= 1e-6), err
+    for sid, got, case in zip(ids, outs[0], cases):
+        assert_components(got, b64.download(sid), 1e-6, gamma=case[2])
     b64.close()
     best = autotune.tune_batch(_capi.FP32, _capi.VANLEER, 100, 100, False, steps=2)
     assert 0 <= best < len(configs)

@@ -8,7 +8,7 @@ import pytest
 from mhd_gpu_solver_b200 import _capi
 from mhd_gpu_solver_b200.batch import state_bytes
 from mhd_gpu_solver_b200.serve import make_stream, serve, serve_one_at_a_time
-from tests.helpers import rel_l1
+from tests.helpers import assert_components
 
 pytestmark = pytest.mark.gpu
 
@@ -30,8 +30,7 @@ def test_served_results_equal_alone_and_fp64_path():
     steps_mixed = {c.rid: c.steps for c in mixed.completions}
     for c in plain.completions:
         assert abs(steps_mixed[c.rid] - c.steps) <= 1
-        err = rel_l1(mixed.states[c.rid], plain.states[c.rid])
-        assert np.all(err[[0, 1, 2, 4, 5, 6]] <= 1e-6), (c.rid, err)
+        assert_components(mixed.states[c.rid], plain.states[c.rid], 1e-6, what=c.rid)
 
 
 def test_admission_respects_the_memory_cap():

@@ -1,12 +1,16 @@
 """Host-side logic without a GPU: the numpy ghost fill and wall fill of the Python surface
 against the oracle, the boundary index maps, and the seeded workload generators."""
 
+import os
+
 import numpy as np
 import pytest
 
 from mhd_gpu_solver_b200 import mhd_solver as ms
 from mhd_gpu_solver_b200 import workloads as wl
 from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 @pytest.mark.parametrize("nx,ny", [(1, 1), (1, 3), (3, 1), (2, 5), (7, 4), (33, 9)])
@@ -137,3 +141,29 @@ def test_bench_traffic_lookup_covers_every_march_tma_kind():
         assert traffic == pytest.approx(s2 * 1000.0) and src
     assert bench.measured_traffic("tile", 2, 1000.0) == (None, None)
     assert bench.BYTES_FORM["march_tma_delta"] == {1: 72.0, 2: 180.0}
+
+
+def test_bench_state_is_the_reference_ghost_fill_and_loads_no_cuda_library():
+    """The bench's 4096^2 state builder (numpy wrap padding) equals embed + the reference's
+    periodic ghost fill, and the reference arm's path (bench.initial_state, the oracle front end)
+    imports no module that loads libmhd_b200.so."""
+    import subprocess
+    import sys
+
+    import bench
+    from mhd_gpu_solver_b200 import workloads as wl
+    from mhd_gpu_solver_b200.mhd_solver import apply_boundary_conditions
+
+    n = 20
+    U = wl.embed(wl.to_conservative(wl.fourier_state(n, n, bench.SEED), bench.GAMMA))
+    apply_boundary_conditions(U, n, n, 2, 0, 0)
+    assert np.array_equal(bench.initial_state(n), U)
+    probe = ("import sys; sys.path.insert(0, %r); import bench; bench.initial_state(8); "
+             "from oracle import oracle; "
+             "print(sorted(m for m in sys.modules if m.startswith('mhd_gpu_solver_b200')))"
+             % ROOT)
+    res = subprocess.run([sys.executable, "-c", probe], capture_output=True, text=True,
+                         timeout=120)
+    assert res.returncode == 0, res.stderr
+    loaded = eval(res.stdout.strip().splitlines()[-1])
+    assert "mhd_gpu_solver_b200._capi" not in loaded, loaded

@@ -70,3 +70,39 @@ def test_periodic_solve_conserves_totals(lim):
     scale = np.abs(interior(U0)).reshape(9, -1).sum(axis=1)
     # rho, momentum, energy and B are conserved (psi is damped)
     assert np.all(np.abs(b - a)[:8] <= 1e-12 * scale[:8])
+
+
+_THREAD_PROBE = """
+import hashlib, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+from mhd_gpu_solver_b200 import workloads as wl
+from oracle import oracle as orc
+from tests.helpers import initial_state
+bc = (orc.OUTFLOW, orc.PERIODIC)
+mask = wl.circles_and_rectangles(67, 45, 2)
+U0 = initial_state(wl.fourier_state(67, 45, 4), 5.0 / 3.0, bc, mask)
+p = orc.Params(limiter=orc.VANLEER, ohmic=True, hall=True, ambipolar=True, eta_ohm=1e-3,
+               eta_hall=1e-2, eta_ambipolar=1e-3, max_steps=12, fixed_steps=True)
+out, t, steps, c_h = orc.solve(U0, orc.Grid(67, 45), p, bc, mask)
+print(hashlib.sha256(out.tobytes()).hexdigest(), t.hex(), steps, c_h.hex())
+"""
+
+
+def test_oracle_results_do_not_depend_on_the_thread_count():
+    """The oracle's loops run on all host threads (OpenMP); every value they write depends only
+    on inputs of the same pass and the CFL maximum is combined per row, so 1 and 3 threads give
+    the same bits."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = []
+    for threads in ("1", "3"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        res = subprocess.run([sys.executable, "-c", _THREAD_PROBE.format(root=root)], env=env,
+                             capture_output=True, text=True, timeout=300)
+        assert res.returncode == 0, res.stderr
+        outs.append(res.stdout.strip())
+    assert outs[0] == outs[1] and outs[0]

@@ -93,3 +93,24 @@ def test_no_alloc_refuses_grids_beyond_its_scratch():
                                                 C.byref(r), None)
     assert rc == _capi.INVALID_ARGUMENT
     assert b"exceeds the 233016-cell limit" in _capi.lib.mhdb_last_error(None)
+
+
+def test_no_alloc_refuses_partly_overlapping_state_buffers():
+    """u_out must equal u_in or lie wholly apart from it. Both pointers here lie inside one
+    allocation twice the state's size, so even an unchecked copy would stay in bounds."""
+    import torch
+
+    if not _capi.cuda_available():
+        pytest.fail("no CUDA device")
+    nx, ny = 40, 30
+    buf = torch.zeros(2 * 9 * nx * ny, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    g = _capi.Grid(nx, ny, 2, 0.0, 1.0, 0.0, 1.0)
+    r = _capi.Result()
+    p = _capi.make_params()
+    base = buf.data_ptr()
+    rc = _capi.lib.mhdb_solve_steps_noalloc_f64(C.byref(g), 0, 0, C.byref(p), 1,
+                                                C.c_void_p(base), C.c_void_p(base + 8 * nx),
+                                                C.byref(r), None)
+    assert rc == _capi.INVALID_ARGUMENT
+    assert b"must equal u_in or not overlap it" in _capi.lib.mhdb_last_error(None)
