@@ -404,13 +404,12 @@ def bench_batched(nsolves: int, steps: int, seed: int = 1) -> dict:
 
     bm, idm, ms_m, launches = run(_capi.FP32)
     b64, id64, ms_64, _ = run(_capi.FP64)
+    from mhd_gpu_solver_b200.accuracy import component_l1
+
     errs = []
     for (nx, ny, g, sd), a, c in zip(solves, idm, id64):
         um, u64 = bm.download(a), b64.download(c)
-        inner = (slice(None), slice(2, -2), slice(2, -2))
-        num = np.abs(um[inner] - u64[inner]).reshape(9, -1).sum(axis=1)
-        den = np.abs(u64[inner]).reshape(9, -1).sum(axis=1)
-        errs.append(float(np.max((num / np.where(den > 0, den, 1.0))[[0, 1, 2, 4, 5, 6]])))
+        errs.append(float(np.max(component_l1(um, u64, b64.status(c)[0].c_h))))
     bm.close()
     b64.close()
     # one at a time through the single-solve FP32-mixed path
@@ -476,9 +475,9 @@ def bench_strips(U: np.ndarray, n: int, steps: int, count: int = 2) -> dict:
         whole = dev.download()[:, 2:-2, 2:-2]
     finally:
         dev.close()
-    num = np.abs(split - whole).reshape(9, -1).sum(axis=1)
-    den = np.abs(whole).reshape(9, -1).sum(axis=1)
-    l1 = num / np.where(den > 0, den, 1.0)
+    from mhd_gpu_solver_b200.accuracy import component_l1
+
+    l1 = component_l1(split, whole, r[2], ng=0)
     cells = float(n) * n * steps
     return {"workload": f"{n}^2 periodic Fourier, FP32-mixed, van Leer, {count} y strips of "
                         f"{n // count} rows + {OVERLAP} overlap rows per side on one GPU, "
@@ -487,30 +486,29 @@ def bench_strips(U: np.ndarray, n: int, steps: int, count: int = 2) -> dict:
             "whole_grid_zone_updates_per_s": cells / (ms_whole * 1e-3),
             "ratio_to_whole_grid": ms_whole / ms,
             "exchange_bytes_per_step": 2 * count * OVERLAP * n * 18 * 4,
-            "l1_vs_whole_grid_max": float(np.max(l1[[0, 1, 2, 4, 5, 6]]))}
+            "l1_vs_whole_grid_max": float(np.max(l1))}
 
 
 def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
-    """The non-ideal, masked workload: n^2, the seeded Fourier state (generated on the device),
-    Ohmic 1e-3, Hall 1e-2, ambipolar 1e-3, 12 circles and 6 rectangles of reflective walls,
-    outflow in x and periodic in y, van Leer, `steps` RK2 steps, FP64 plain vs FP32-mixed (both
-    on their masked default kernels: FP64 the shared-memory tile kernel, FP32-mixed the masked
-    TMA strip march). Reports each form's zone-updates/s, the
-    FP32-mixed L1 error against the FP64 result, and the FP64 div-B norms and mass/energy
-    drift."""
+    """The non-ideal, masked workload: n^2, the seeded Fourier state and mask (both generated on
+    the device), Ohmic 1e-3, Hall 1e-2, ambipolar 1e-3, 12 circles and 6 rectangles of reflective
+    walls, outflow in x and periodic in y, van Leer, `steps` RK2 steps, FP64 plain vs FP32-mixed
+    (both on their masked default kernels, the masked TMA strip marches). Reports each form's
+    zone-updates/s, the FP32-mixed L1 error against the FP64 result (every component), and the
+    FP64 div-B norms and mass/energy drift."""
     import torch
 
     from mhd_gpu_solver_b200 import _capi
     from mhd_gpu_solver_b200 import workloads as wl
 
-    mask = wl.circles_and_rectangles(n, n, seed)
+    shapes = wl.circles_and_rectangles_shapes(seed)  # rasterised on the device
     params = _capi.make_params(limiter=_capi.VANLEER, ohmic=True, hall=True, ambipolar=True,
                                eta_ohm=1e-3, eta_hall=1e-2, eta_ambipolar=1e-3)
     out, states = {}, {}
     for name, prec in (("fp64", _capi.FP64), ("fp32_mixed", _capi.FP32)):
         dev = _capi.DeviceSolver(n, n, precision=prec)
         try:
-            dev.configure(_capi.BC_OUTFLOW, _capi.BC_PERIODIC, mask, True)
+            dev.configure_shapes(_capi.BC_OUTFLOW, _capi.BC_PERIODIC, shapes, True)
             dev.generate(_capi.InitSpec.fourier(seed), params)
             d0 = dev.diagnostics(params)
             dev.solve_steps(params, 40)  # warm-up: kernel attributes, the 32-step graph batch
@@ -525,6 +523,8 @@ def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
             ms = e0.elapsed_time(e1)
             d1 = dev.diagnostics(params)
             states[name] = dev.download()
+            if name == "fp64":
+                c_h64 = r.c_h
         finally:
             dev.close()
         out[name] = {"zone_updates_per_s": float(n) * n * steps / (ms * 1e-3), "ms": ms,
@@ -532,15 +532,13 @@ def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
                      "div_b_l2": d1["div_b_l2"], "div_b_max": d1["div_b_max"],
                      "mass_drift": (d1["mass"] - d0["mass"]) / d0["mass"],
                      "energy_drift": (d1["energy"] - d0["energy"]) / d0["energy"]}
-    inner = (slice(None), slice(2, -2), slice(2, -2))
-    a, b = states["fp32_mixed"][inner], states["fp64"][inner]
-    num = np.abs(a - b).reshape(9, -1).sum(axis=1)
-    den = np.abs(b).reshape(9, -1).sum(axis=1)
-    l1 = num / np.where(den > 0, den, 1.0)
+    from mhd_gpu_solver_b200.accuracy import component_l1
+
+    l1 = component_l1(states["fp32_mixed"], states["fp64"], c_h64)
     out["workload"] = (f"{n}^2 masked (12 circles, 6 rectangles, reflective walls), Ohmic/Hall/"
                        f"ambipolar 1e-3/1e-2/1e-3, outflow x, periodic y, van Leer, {steps} steps")
     out["speedup_fp32_mixed_over_fp64"] = out["fp64"]["ms"] / out["fp32_mixed"]["ms"]
-    out["l1_fp32_mixed_vs_fp64_max"] = float(np.max(l1[[0, 1, 2, 4, 5, 6]]))
+    out["l1_fp32_mixed_vs_fp64_max"] = float(np.max(l1))
     return out
 
 

@@ -121,6 +121,27 @@ int mhdb_precision(const mhdb_solver* h);
 int mhdb_configure(mhdb_solver* h, int bc_x, int bc_y, const uint8_t* mask, size_t mask_len,
                    int reflective_walls);
 
+/* Additive: configure with a mask rasterised on the device from circles and rectangles instead of
+   a host array (no host mask, no upload). The rule of the reference's geometry helpers
+   (gui/geometry.py:22-38, :130-156): every interior cell starts fluid; the shapes are applied in
+   order, each painting the cells whose centre x_min + (i + 1/2) dx, y_min + (j + 1/2) dy it
+   contains solid (solid = 1) or fluid (solid = 0), later shapes overwriting earlier ones; a circle
+   contains (x - a)^2 + (y - b)^2 <= c^2, a rectangle min(a, c) <= x <= max(a, c) and
+   min(b, d) <= y <= max(b, d), both inclusive. The mask equals the host rasterisation of the same
+   shapes bit for bit. count may be 0 (all fluid). */
+enum { MHDB_SHAPE_CIRCLE = 0, MHDB_SHAPE_RECTANGLE = 1 };
+typedef struct mhdb_shape {
+    int kind;          /* MHDB_SHAPE_CIRCLE or MHDB_SHAPE_RECTANGLE */
+    int solid;         /* 1: contained cells become solid; 0: fluid */
+    double a, b, c, d; /* circle: centre (a, b), radius c; rectangle: corners (a, b), (c, d) */
+} mhdb_shape;
+int mhdb_configure_shapes(mhdb_solver* h, int bc_x, int bc_y, const mhdb_shape* shapes, int count,
+                          int reflective_walls);
+
+/* Additive: the interior fluid mask the handle uses (MHDSolver::mask(), the reference module's
+   get_mask), row-major ny * nx bytes, 1 = fluid; len must be nx * ny. */
+int mhdb_get_mask(mhdb_solver* h, uint8_t* out, size_t len);
+
 /* DeviceSolver::upload / download (device_solver.hpp:70-71): nine host planes of n_tot =
    (nx + 2 ng)(ny + 2 ng) doubles each. download returns the state with ghosts filled by the
    boundary rule and solid cells wall-filled, as the reference's solve() leaves it. */

@@ -33,7 +33,8 @@ EXPORTS = (
     "mhdb_batch_launch", "mhdb_batch_poll", "mhdb_batch_config_count", "mhdb_batch_config_info",
     "mhdb_batch_set_config", "mhdb_set_cell_size", "mhdb_set_reduce_rows", "mhdb_strip_view", "mhdb_strip_begin",
     "mhdb_strip_step", "mhdb_strip_finish", "mhdb_strip_poll", "mhdb_strip_end",
-    "mhdb_debug_stall_copies", "mhdb_batch_debug_stall_copies",
+    "mhdb_debug_stall_copies", "mhdb_batch_debug_stall_copies", "mhdb_configure_shapes",
+    "mhdb_get_mask",
 )
 
 
@@ -65,6 +66,13 @@ class Diag(C.Structure):
     _fields_ = [("mass", C.c_double), ("energy", C.c_double), ("div_b_max", C.c_double),
                 ("div_b_l2", C.c_double), ("rho_min", C.c_double), ("p_min", C.c_double),
                 ("finite", C.c_int)]
+
+
+class Shape(C.Structure):
+    """mhdb_shape: kind 0 circle (centre (a, b), radius c), 1 rectangle (corners (a, b),
+    (c, d)); solid 1 paints contained cells solid, 0 fluid."""
+    _fields_ = [("kind", C.c_int), ("solid", C.c_int), ("a", C.c_double), ("b", C.c_double),
+                ("c", C.c_double), ("d", C.c_double)]
 
 
 class StripState(C.Structure):
@@ -115,6 +123,9 @@ def _load() -> C.CDLL:
         "mhdb_tile_config_kind": ([C.c_int, C.c_int], C.c_int),
         "mhdb_set_tile_config": ([h, C.c_int], C.c_int),
         "mhdb_debug_stall_copies": ([h, C.c_int], C.c_int),
+        "mhdb_configure_shapes": ([h, C.c_int, C.c_int, C.POINTER(Shape), C.c_int, C.c_int],
+                                  C.c_int),
+        "mhdb_get_mask": ([h, C.POINTER(C.c_uint8), C.c_size_t], C.c_int),
         "mhdb_solve_steps_noalloc_f64": ([C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(Params),
                                           C.c_int, C.c_void_p, C.c_void_p, C.POINTER(Result),
                                           C.c_void_p], C.c_int),
@@ -244,6 +255,23 @@ class DeviceSolver:
                                     m.ctypes.data_as(C.POINTER(C.c_uint8)), m.size,
                                     int(reflective_walls))
         raise_for(rc, self._h)
+
+    def configure_shapes(self, bc_x: int, bc_y: int, shapes, reflective_walls: bool = True) -> None:
+        """configure() with a mask rasterised on the device from (kind, solid, a, b, c, d)
+        shapes (workloads.circles_and_rectangles_shapes), painted in order."""
+        arr = (Shape * max(1, len(shapes)))(*[Shape(int(k), int(sd), float(a), float(b),
+                                                    float(c), float(d))
+                                              for k, sd, a, b, c, d in shapes])
+        raise_for(lib.mhdb_configure_shapes(self._h, int(bc_x), int(bc_y), arr, len(shapes),
+                                            int(reflective_walls)), self._h)
+
+    def get_mask(self) -> np.ndarray:
+        """The interior fluid mask in use, (ny, nx) uint8, 1 = fluid."""
+        ny, nx = self.shape[1] - 2 * self.ng, self.shape[2] - 2 * self.ng
+        out = np.empty((ny, nx), dtype=np.uint8)
+        raise_for(lib.mhdb_get_mask(self._h, out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size),
+                  self._h)
+        return out
 
     def upload(self, state: np.ndarray) -> None:
         ptrs = plane_pointers(state)

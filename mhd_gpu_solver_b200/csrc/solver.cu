@@ -19,6 +19,7 @@
 #include "stage_mixed.cuh"
 #include "diagnostics.cuh"
 #include "generate.cuh"
+#include "mask_gen.cuh"
 #include "stage_select.h"
 
 #include <cuda_runtime.h>
@@ -229,6 +230,7 @@ struct mhdb_solver {
     uint8_t* mask = nullptr;
     Ctrl* ctrl = nullptr;
     Ctrl* ctrl_host = nullptr;
+    int* flag = nullptr;         // device int of the mask rasteriser (any solid cell)
     double* diag = nullptr;      // kDiagFields * kDiagBlocks partials + kDiagFields results
     double* diag_host = nullptr; // pinned copy of the results
 
@@ -726,6 +728,7 @@ void release(mhdb_solver* h)
     if (h->ctrl) cudaFree(h->ctrl);
     if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
     if (h->diag) cudaFree(h->diag);
+    if (h->flag) cudaFree(h->flag);
     if (h->diag_host) cudaFreeHost(h->diag_host);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -950,6 +953,74 @@ int mhdb_configure(mhdb_solver* h, int bc_x, int bc_y, const uint8_t* mask, size
                                          h->grid.ny, cudaMemcpyHostToDevice, h->stream));
             MHDB_CHECK(cudaStreamSynchronize(h->stream));
         }
+    });
+}
+
+int mhdb_configure_shapes(mhdb_solver* h, int bc_x, int bc_y, const mhdb_shape* shapes, int count,
+                          int reflective_walls)
+{
+    return guarded(h, [&] {
+        if (bc_x == kReflective || bc_y == kReflective) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "Reflective boundary conditions are not implemented yet"};
+        }
+        if ((bc_x != kPeriodic && bc_x != kOutflow) || (bc_y != kPeriodic && bc_y != kOutflow)) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "unknown boundary condition type"};
+        }
+        if (count < 0 || (count > 0 && shapes == nullptr)) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "shapes must not be NULL when count > 0"};
+        }
+        for (int k = 0; k < count; ++k) {
+            if (shapes[k].kind != MHDB_SHAPE_CIRCLE && shapes[k].kind != MHDB_SHAPE_RECTANGLE) {
+                throw ApiError{MHDB_INVALID_ARGUMENT, "unknown shape kind"};
+            }
+        }
+        if (h->flag == nullptr) {
+            MHDB_CHECK(cudaMalloc(reinterpret_cast<void**>(&h->flag), sizeof(int)));
+        }
+        ShapeList L{};
+        L.x_min = h->grid.x_min;
+        L.dx = (h->grid.x_max - h->grid.x_min) / static_cast<double>(h->grid.nx);
+        L.y_min = h->grid.y_min;
+        L.dy = (h->grid.y_max - h->grid.y_min) / static_cast<double>(h->grid.ny);
+        const long long n = static_cast<long long>(h->grid.nx) * h->grid.ny;
+        int k0 = 0;
+        do { // at least one launch: count == 0 leaves an all-fluid mask
+            L.count = std::min(count - k0, kShapesPerLaunch);
+            L.first = k0 == 0 ? 1 : 0;
+            for (int k = 0; k < L.count; ++k) {
+                L.s[k] = shapes[k0 + k];
+            }
+            // every launch rewrites and checks every cell, so the last one's flag holds
+            MHDB_CHECK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+            rasterize_shapes<<<launch_blocks(n, 256), 256, 0, h->stream>>>(h->mask, h->geom, L,
+                                                                           h->flag);
+            ++h->launches;
+            MHDB_CHECK(cudaGetLastError());
+            k0 += L.count;
+        } while (k0 < count);
+        int any = 0;
+        MHDB_CHECK(cudaMemcpyAsync(&any, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
+        h->geom.bc_x = bc_x;
+        h->geom.bc_y = bc_y;
+        h->walls = reflective_walls != 0;
+        h->has_mask = any != 0;
+    });
+}
+
+int mhdb_get_mask(mhdb_solver* h, uint8_t* out, size_t len)
+{
+    return guarded(h, [&] {
+        if (out == nullptr || len != static_cast<size_t>(h->grid.nx) * h->grid.ny) {
+            throw ApiError{MHDB_INVALID_ARGUMENT, "FluidMask size does not match Grid2D interior"};
+        }
+        if (!h->has_mask) {
+            std::memset(out, 1, len);
+            return;
+        }
+        MHDB_CHECK(cudaMemcpy2DAsync(out, h->grid.nx, h->mask, h->geom.pitch, h->grid.nx,
+                                     h->grid.ny, cudaMemcpyDeviceToHost, h->stream));
+        MHDB_CHECK(cudaStreamSynchronize(h->stream));
     });
 }
 

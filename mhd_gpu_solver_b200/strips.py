@@ -134,17 +134,12 @@ class _Comm:
         d = self.dist
         sends = sorted(sends, key=lambda m: (m[0], m[1]))
         recvs = sorted(recvs, key=lambda m: (m[0], m[1]))
-        if d.get_backend(self.group) == "nccl":
-            # one NCCL group: sends and receives to the same peer cannot wait on each other
-            ops = [d.P2POp(d.isend, t, self.global_rank(p), self.group, tag)
-                   for p, tag, t in sends]
-            ops += [d.P2POp(d.irecv, t, self.global_rank(p), self.group, tag)
-                    for p, tag, t in recvs]
-            works = d.batch_isend_irecv(ops)
-        else:
-            works = [d.isend(t, self.global_rank(p), self.group, tag) for p, tag, t in sends]
-            works += [d.irecv(t, self.global_rank(p), self.group, tag) for p, tag, t in recvs]
-        for w in works:
+        # One batch for every backend (NCCL runs it as one group, so sends and receives to the
+        # same peer cannot wait on each other; gloo matches the tags): the CPU tests run the code
+        # path the GPUs run.
+        ops = [d.P2POp(d.isend, t, self.global_rank(p), self.group, tag) for p, tag, t in sends]
+        ops += [d.P2POp(d.irecv, t, self.global_rank(p), self.group, tag) for p, tag, t in recvs]
+        for w in d.batch_isend_irecv(ops):
             w.wait()
 
     def gather_objects(self, obj) -> list:

@@ -150,23 +150,52 @@ def fourier_state(nx: int, ny: int, seed: int = 0, kmax: int = 8, x_min=0.0, x_m
     return out
 
 
+CIRCLE, RECTANGLE = 0, 1  # shape kinds of the C ABI (mhdb_shape)
+
+
+def circles_and_rectangles_shapes(seed: int = 0, n_circles: int = 12,
+                                  n_rects: int = 6) -> list[tuple]:
+    """The seeded shapes of the masked workload as (kind, solid, a, b, c, d) tuples, painted in
+    order: circles (centre (a, b) ~ U[0,1]^2, radius c ~ U[0.02, 0.08]), then rectangles (lower
+    left corner (a, b) ~ U[0,1]^2, upper right corner (a + w, b + h), w and h ~ U[0.02, 0.15]),
+    all solid."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shapes = []
+    for _ in range(n_circles):
+        cx, cy = rng.uniform(0.0, 1.0, size=2)
+        r = rng.uniform(0.02, 0.08)
+        shapes.append((CIRCLE, 1, float(cx), float(cy), float(r), 0.0))
+    for _ in range(n_rects):
+        x0, y0 = rng.uniform(0.0, 1.0, size=2)
+        w, h = rng.uniform(0.02, 0.15, size=2)
+        shapes.append((RECTANGLE, 1, float(x0), float(y0), float(x0 + w), float(y0 + h)))
+    return shapes
+
+
+def rasterize(shapes, nx: int, ny: int, x_min=0.0, x_max=1.0, y_min=0.0,
+              y_max=1.0) -> np.ndarray:
+    """Interior fluid mask (ny, nx), 1 = fluid, by the rule of the reference's geometry helpers
+    (gui/geometry.py:22-38, :130-156): all fluid, then each shape in order paints the cells whose
+    centre it contains (inclusive tests), later shapes overwriting earlier ones."""
+    xs, ys = cell_centers(nx, ny, x_min, x_max, y_min, y_max)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")
+    mask = np.ones((ny, nx), dtype=np.uint8)
+    for kind, solid, a, b, c, d in shapes:
+        if kind == CIRCLE:
+            hit = (X - a) ** 2 + (Y - b) ** 2 <= c * c
+        else:
+            xa, xb = sorted((a, c))
+            ya, yb = sorted((b, d))
+            hit = (X >= xa) & (X <= xb) & (Y >= ya) & (Y <= yb)
+        mask[hit] = 0 if solid else 1
+    return mask
+
+
 def circles_and_rectangles(nx: int, ny: int, seed: int = 0, n_circles: int = 12,
                            n_rects: int = 6) -> np.ndarray:
     """Circles: centre ~ U[0,1]^2, radius ~ U[0.02, 0.08]; rectangles: lower-left corner
     ~ U[0,1]^2, width and height ~ U[0.02, 0.15]. Circles first, then rectangles."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    xs, ys = cell_centers(nx, ny)
-    X, Y = np.meshgrid(xs, ys, indexing="xy")
-    mask = np.ones((ny, nx), dtype=np.uint8)
-    for _ in range(n_circles):
-        cx, cy = rng.uniform(0.0, 1.0, size=2)
-        r = rng.uniform(0.02, 0.08)
-        mask[(X - cx) ** 2 + (Y - cy) ** 2 <= r * r] = 0
-    for _ in range(n_rects):
-        x0, y0 = rng.uniform(0.0, 1.0, size=2)
-        w, h = rng.uniform(0.02, 0.15, size=2)
-        mask[(X >= x0) & (X <= x0 + w) & (Y >= y0) & (Y <= y0 + h)] = 0
-    return mask
+    return rasterize(circles_and_rectangles_shapes(seed, n_circles, n_rects), nx, ny)
 
 
 def orszag_tang(nx: int, ny: int) -> dict:

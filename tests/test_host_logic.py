@@ -167,3 +167,32 @@ def test_bench_state_is_the_reference_ghost_fill_and_loads_no_cuda_library():
     assert res.returncode == 0, res.stderr
     loaded = eval(res.stdout.strip().splitlines()[-1])
     assert "mhd_gpu_solver_b200._capi" not in loaded, loaded
+
+
+def test_host_rasterize_follows_the_reference_rule_cell_by_cell():
+    """workloads.rasterize against a per-cell restatement of gui/geometry.py:22-38 (contains:
+    inclusive circle and rectangle tests, rectangle corners sorted) and :130-156 (rasterize: all
+    fluid, shapes in order, later ones overwrite), on shapes whose edges pass through cell
+    centres."""
+    nx, ny = 10, 8
+    shapes = [(wl.RECTANGLE, 1, 0.45, 0.0625, 0.05, 0.5625),  # corners reversed; edges on centres
+              (wl.CIRCLE, 1, 0.75, 0.5, 0.2, 0.0),
+              (wl.CIRCLE, 0, 0.75, 0.5, 0.1, 0.0),           # fluid paint inside the solid disc
+              (wl.RECTANGLE, 0, 0.25, 0.3125, 0.35, 0.3125)]  # a one-row fluid strip
+    got = wl.rasterize(shapes, nx, ny)
+    xs, ys = wl.cell_centers(nx, ny)
+    want = np.ones((ny, nx), dtype=np.uint8)
+    for j in range(ny):
+        for i in range(nx):
+            x, y = float(xs[i]), float(ys[j])
+            for kind, solid, a, b, c, d in shapes:
+                if kind == wl.CIRCLE:
+                    hit = (x - a) ** 2 + (y - b) ** 2 <= c ** 2
+                else:
+                    hit = min(a, c) <= x <= max(a, c) and min(b, d) <= y <= max(b, d)
+                if hit:
+                    want[j, i] = 0 if solid else 1
+    assert np.array_equal(got, want)
+    # the strip's row is row 2 (y = 0.3125); its x range [0.25, 0.35] holds the centre 0.25 but
+    # not 0.35000000000000003 (= 0.05 + 3 x 0.1 rounded), so one cell turns fluid
+    assert (got == 0).any() and got[2, 2] == 1 and got[2, 3] == 0
