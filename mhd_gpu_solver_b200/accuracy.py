@@ -12,6 +12,14 @@ bx, by, bz, psi):
   smooth, nearly divergence-free states psi starts at zero and stays at the rounding level of that
   scale, where sum|b| alone would measure rounding rather than agreement; where psi is large
   (shocked states) the rule is the plain relative L1.
+
+With ``vector_scale`` (the rule of the FP32-mixed bar) the components of the momentum and the
+magnetic field are held on their vector's scale: sum|a_c - b_c| / sum|b_vec| with |b_vec| the
+Euclidean norm of m (for m_x, m_y, m_z) or of B (for B_x, B_y, B_z) per cell. A component that is
+a small part of its vector is then held to the accuracy of the vector, not of itself: with a Hall
+term, B_z and m_z are generated from zero by a second derivative of B (the curl of
+eta_H J x B / |B|, J itself a difference of B), which FP32 differencing at fine grids resolves only
+to about eps_FP32 / (k dx)^2 relative to B_z itself.
 """
 
 from __future__ import annotations
@@ -21,7 +29,8 @@ import numpy as np
 COMPONENTS = ("rho", "mx", "my", "mz", "energy", "bx", "by", "bz", "psi")
 
 
-def component_l1(a: np.ndarray, b: np.ndarray, c_h: float, ng: int = 2) -> np.ndarray:
+def component_l1(a: np.ndarray, b: np.ndarray, c_h: float, ng: int = 2,
+                 vector_scale: bool = False) -> np.ndarray:
     """L1 error of a against b per component (9 values), by the rule above."""
     ai = a[:, ng:a.shape[1] - ng, ng:a.shape[2] - ng]
     bi = b[:, ng:b.shape[1] - ng, ng:b.shape[2] - ng]
@@ -32,4 +41,8 @@ def component_l1(a: np.ndarray, b: np.ndarray, c_h: float, ng: int = 2) -> np.nd
         den[c] = float(np.abs(bi[c]).sum())
     bmag = float(np.sqrt(bi[5] * bi[5] + bi[6] * bi[6] + bi[7] * bi[7]).sum())
     den[8] = max(den[8], float(c_h) * bmag)
+    if vector_scale:
+        mmag = float(np.sqrt(bi[1] * bi[1] + bi[2] * bi[2] + bi[3] * bi[3]).sum())
+        den[1:4] = mmag
+        den[5:8] = bmag
     return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)

@@ -3,8 +3,9 @@
 Tolerances: the plain FP64 form must match the oracle to relative L1 <= 1e-12 per conserved
 component after the stated step count, with the same step count (the FP64 parity bar), and the
 mask must be handled the same way. The FP32-mixed form is held to relative L1 <= 1e-6. Every one
-of the nine components is held (tests.helpers.component_errors): components whose reference value
-is identically zero in absolute L1, psi on the scale max(sum|psi|, c_h sum|B|).
+of the nine components is held (tests.helpers.assert_components): components whose reference value
+is identically zero in absolute L1, psi on the scale max(sum|psi|, c_h sum|B|), and under the
+FP32-mixed bar the components of m and B on their vector's scale.
 """
 
 import json
