@@ -93,6 +93,8 @@ def parse():
     ap.add_argument("--serve-plain-sample", type=int, default=0,
                     help="time the one-at-a-time FP64 path on this many seeded requests of the "
                          "stream and estimate the whole stream from them (0: run it all)")
+    ap.add_argument("--serve-log", default=None,
+                    help="file that receives one JSON line per finished served request")
     ap.add_argument("--accuracy-steps", type=int, default=500,
                     help="steps of the FP32-mixed vs FP64 L1 check at the headline size (0 skips)")
     return ap.parse_args()
@@ -548,35 +550,51 @@ def bench_masked_nonideal(n: int, steps: int, seed: int = 3) -> dict:
     return out
 
 
-def bench_served(nreq: int, side, tend, rate: float, plain_sample: int = 0) -> dict:
+def bench_served(nreq: int, side, tend, rate: float, plain_sample: int = 0,
+                 log_path: str | None = None) -> dict:
     """The served stream: seeded Poisson arrivals at `rate`, FP32-mixed continuous batching
     under the 150 GB cap, against the plain FP64 path one request at a time. With plain_sample >
-    0 the plain path runs a seeded random subsample of that many requests and its time for the
-    whole stream is estimated by a least-squares fit of per-request seconds = a + b x
-    zone-updates over the sample, summed over every request (the plain path's requests run back
-    to back at a saturating rate, so its makespan is that sum)."""
+    0 the plain path runs a seeded random subsample of that many requests (first, back to back)
+    and its time for the whole stream is estimated by a least-squares fit of per-request seconds
+    = a + b x zone-updates over the sample, summed over every request (the plain path's requests
+    run back to back at a saturating rate, so its makespan is that sum). log_path: one JSON line
+    per finished request (and the plain estimate), written as the run goes."""
     from mhd_gpu_solver_b200.serve import make_stream, prepare, serve, serve_one_at_a_time
 
+    log = open(log_path, "a", buffering=1) if log_path else None
+
+    def note(obj):
+        if log is not None:
+            log.write(json.dumps(obj) + "\n")
+
     stream = make_stream(nreq, rate=rate, seed=2, side=side, t_end=tend, nonideal_frac=0.3)
-    prepare(stream)  # batch autotuning of the stream's size classes, outside the timed run
-    stats = serve(stream)
-    served = stats.summary()
-    work = {c.rid: c.cells * c.steps for c in stats.completions}
     out = {"workload": f"{nreq} requests, Poisson arrivals at {rate:g}/s, side "
                        f"log-uniform in [{side[0]},{side[1]}], t_end ~ U[{tend[0]},{tend[1]}], "
-                       "Fourier or four-quadrant 50/50, 30% non-ideal, FP32-mixed, 150 GB cap",
-           "served": served}
-    if plain_sample <= 0 or plain_sample >= nreq:
+                       "Fourier or four-quadrant 50/50, 30% non-ideal, FP32-mixed, 150 GB cap"}
+    sample = None
+    if 0 < plain_sample < nreq:
+        import copy
+
+        rng = np.random.Generator(np.random.PCG64(11))
+        pick = sorted(rng.choice(nreq, size=plain_sample, replace=False).tolist())
+        sample = [copy.copy(stream[i]) for i in pick]
+        for r in sample:
+            r.arrival = 0.0  # back to back: the plain path is the bottleneck at a saturating rate
+        ps = serve_one_at_a_time(sample)
+        note({"plain_sample_done": plain_sample, "seconds": ps.makespan})
+    prepare(stream)  # batch autotuning of the stream's size classes, outside the timed run
+    stats = serve(stream, on_complete=lambda c, st: note(
+        {"rid": c.rid, "n": int(round(c.cells ** 0.5)), "steps": c.steps, "arrival": c.arrival,
+         "finished": c.finished, "latency_s": c.latency, "done": len(st.completions)}))
+    served = stats.summary()
+    out["served"] = served
+    note({"served": served})
+    if sample is None:
         plain = serve_one_at_a_time(stream).summary()
         out["one_at_a_time_fp64"] = plain
         out["solves_per_s_ratio"] = served["solves_per_s"] / plain["solves_per_s"]
         return out
-    rng = np.random.Generator(np.random.PCG64(11))
-    pick = sorted(rng.choice(nreq, size=plain_sample, replace=False).tolist())
-    sample = [stream[i] for i in pick]
-    for r in sample:
-        r.arrival = 0.0  # back to back: the plain path is the bottleneck at a saturating rate
-    ps = serve_one_at_a_time(sample)
+    work = {c.rid: c.cells * c.steps for c in stats.completions}
     secs = np.array([c.finished - c.admitted for c in ps.completions])
     zu = np.array([float(work[c.rid]) for c in ps.completions])
     A = np.stack([np.ones_like(zu), zu], axis=1)
@@ -590,6 +608,7 @@ def bench_served(nreq: int, side, tend, rate: float, plain_sample: int = 0) -> d
         "sample_zone_updates": float(zu.sum()), "fit_a_s": float(a), "fit_b_s": float(b),
         "estimated_makespan_s": est, "solves_per_s": nreq / est}
     out["solves_per_s_ratio"] = served["solves_per_s"] / (nreq / est)
+    note({"result": out})
     return out
 
 
@@ -791,7 +810,7 @@ def main():
         side = tuple(int(v) for v in args.serve_side.split(","))
         tend = tuple(float(v) for v in args.serve_tend.split(","))
         line["served"] = bench_served(args.serve_requests, side, tend, args.serve_rate,
-                                      args.serve_plain_sample)
+                                      args.serve_plain_sample, args.serve_log)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference_rate(U, n, args.cpu_steps)

@@ -160,9 +160,10 @@ def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
 
 def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
           chunk: int = 16, download: bool = True, keep_states: bool = False,
-          tune: bool = True) -> ServeStats:
+          tune: bool = True, on_complete=None) -> ServeStats:
     """Serve a request stream in real time with continuous batching. tune: each request runs
-    the batch configuration tuned for its size class (see prepare)."""
+    the batch configuration tuned for its size class (see prepare). on_complete(completion,
+    stats) is called after each request finishes (progress records of long streams)."""
     batch = BatchSolver(precision, tune=tune)
     stats = ServeStats()
     results = ResultBuffer()
@@ -207,6 +208,8 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
                 stats.completions.append(Completion(req.rid, req.arrival, admitted,
                                                     time.perf_counter() - start if download
                                                     else polled, r.steps, r.t, req.n * req.n))
+                if on_complete is not None:
+                    on_complete(stats.completions[-1], stats)
                 batch.remove(sid)
                 in_use -= state_bytes(req.n, req.n)
             done = []
