@@ -186,11 +186,12 @@ long long mhdb_launch_count(const mhdb_solver* h);
    mhdb_tile_config_kind returns its kernel: MHDB_KERNEL_TILE (shared-memory tile, separate x and
    y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp strip march, 28
    columns per warp), MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
-   memory) or MHDB_KERNEL_MARCH_TMA_DELTA (the same for the FP32-mixed increment form: stage 1
-   stores the FP32 increment dt L instead of U*, stage 2 reads U^n + increment),
+   memory), MHDB_KERNEL_MARCH_TMA_DELTA (the same for the FP32-mixed increment form: stage 1
+   stores the FP32 increment dt L instead of U*, stage 2 reads U^n + increment) or
+   MHDB_KERNEL_MARCH_TMA_PAIR (the increment form with two columns per lane, 60 columns per warp),
    or -1 for an unknown configuration. */
 enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,
-       MHDB_KERNEL_MARCH_TMA = 3, MHDB_KERNEL_MARCH_TMA_DELTA = 4 };
+       MHDB_KERNEL_MARCH_TMA = 3, MHDB_KERNEL_MARCH_TMA_DELTA = 4, MHDB_KERNEL_MARCH_TMA_PAIR = 5 };
 int mhdb_tile_config_count(int precision);
 int mhdb_tile_config_info(int precision, int config, int* tile_x, int* tile_y, int* threads,
                           int* min_blocks);

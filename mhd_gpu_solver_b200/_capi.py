@@ -364,7 +364,8 @@ class DeviceSolver:
         return r
 
 
-KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma", 4: "march_tma_delta"}
+KERNEL_KINDS = {0: "tile", 1: "tile_merged", 2: "march", 3: "march_tma", 4: "march_tma_delta",
+                5: "march_tma_pair"}
 
 
 def tile_configs(precision: int) -> list[dict]:

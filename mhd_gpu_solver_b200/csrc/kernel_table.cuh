@@ -4,6 +4,7 @@
 #include <type_traits>
 
 #include "march_kernel.cuh"
+#include "march_pair.cuh"
 #include "march_tma.cuh"
 #include "stage_kernel.cuh"
 #include "stage_select.h"
@@ -55,6 +56,19 @@ struct MarchTmaCfg {
     static constexpr bool MARCH_TMA = true;
 };
 
+// Two-column TMA strip march of the increment form (march_pair.cuh): one warp per block, LY rows
+// per warp, MINB blocks per SM.
+template <int LY_, int MINB_>
+struct MarchPairCfg {
+    static constexpr int LY = LY_, MINB = MINB_;
+    static constexpr bool MARCH_PAIR = true;
+};
+
+template <class Cfg, class = void>
+struct is_march_pair : std::false_type {};
+template <class Cfg>
+struct is_march_pair<Cfg, std::void_t<decltype(Cfg::MARCH_PAIR)>> : std::true_type {};
+
 template <class Cfg, class = void>
 struct is_march_tma : std::false_type {};
 template <class Cfg>
@@ -68,7 +82,20 @@ struct is_march<Cfg, std::void_t<decltype(Cfg::MARCH)>> : std::true_type {};
 template <class Policy, class Cfg, int L, bool NI, bool MASK>
 void fill_pair(StageKernels& k)
 {
-    if constexpr (is_march_tma<Cfg>::value) {
+    if constexpr (is_march_pair<Cfg>::value) {
+        static_assert(!MASK, "the two-column strip march serves unmasked solves");
+        static_assert(sizeof(typename Policy::T) == 4, "the two-column strip march is FP32-mixed");
+        k.dx_tma1 = march_pair_kernel<L, 1, Cfg::LY, Cfg::MINB, NI>;
+        k.dx_tma2 = march_pair_kernel<L, 2, Cfg::LY, Cfg::MINB, NI>;
+        k.tile_x = kPairOwned;
+        k.tile_y = Cfg::LY;
+        k.threads = 32;
+        k.smem = march_pair_smem_bytes<1>();
+        k.smem2 = march_pair_smem_bytes<2>();
+        k.halo_w = kPairHaloW;
+        k.own_w = kPairOwnW;
+        return;
+    } else if constexpr (is_march_tma<Cfg>::value) {
         static_assert(!MASK || (Cfg::ST1 == 0 && Cfg::ST2 == 0),
                       "masked TMA strip marches store through the lanes");
         constexpr int E = static_cast<int>(sizeof(typename Policy::T));
@@ -153,7 +180,7 @@ StageKernels select_unmasked(int lim, bool ni, bool mask)
     if (mask) {
         return k;
     }
-    if constexpr (is_march<Cfg>::value || is_march_tma<Cfg>::value) {
+    if constexpr (is_march<Cfg>::value || is_march_tma<Cfg>::value || is_march_pair<Cfg>::value) {
 #define MHDB_SEL(LL)                                                                               \
     if (ni) fill_pair<Policy, Cfg, LL, true, false>(k);                                            \
     else fill_pair<Policy, Cfg, LL, false, false>(k);

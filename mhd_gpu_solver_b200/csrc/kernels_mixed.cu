@@ -19,6 +19,8 @@ using Cfg11 = MarchTmaCfg<1, 32, 16, true, 0>;
 using Cfg12 = MarchTmaCfg<1, 64, 16>;
 using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, true>; // increment form (also masked)
 using Cfg14 = MarchTmaCfg<1, 64, 16, true, 0, 0, true>; // increment form, 64-row segments
+using Cfg15 = MarchPairCfg<32, 8>;  // increment form, two columns per lane
+using Cfg16 = MarchPairCfg<32, 10>; // the same, 10 blocks per SM requested (168 registers)
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
@@ -27,7 +29,8 @@ constexpr TileConfigInfo kInfo[] = {
     {56, 32, 64, 8, kKindMarchTma},    {28, 32, 32, 16, kKindMarchTma},
     {112, 32, 128, 4, kKindMarchTma},  {28, 32, 32, 16, kKindMarchTma},
     {28, 64, 32, 16, kKindMarchTma},   {28, 32, 32, 16, kKindMarchTmaDelta},
-    {28, 64, 32, 16, kKindMarchTmaDelta}};
+    {28, 64, 32, 16, kKindMarchTmaDelta}, {60, 32, 32, 8, kKindMarchTmaPair},
+    {60, 32, 32, 10, kKindMarchTmaPair}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -75,6 +78,10 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_full<PolicyMixed, Cfg13>(limiter, nonideal, mask);
     case 14:
         return select_unmasked<PolicyMixed, Cfg14>(limiter, nonideal, mask);
+    case 15:
+        return select_unmasked<PolicyMixed, Cfg15>(limiter, nonideal, mask);
+    case 16:
+        return select_unmasked<PolicyMixed, Cfg16>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

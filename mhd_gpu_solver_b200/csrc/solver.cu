@@ -450,7 +450,7 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
                 s.c2[q] = s.c1[q];
                 std::string err;
                 if (!encode_march_maps_delta(bufs[q], h->delta, h->geom, &s.dm1[q], &s.dm2[q],
-                                             &err)) {
+                                             &err, sk.halo_w, sk.own_w)) {
                     throw ApiError{MHDB_CUDA_ERROR, err};
                 }
             }

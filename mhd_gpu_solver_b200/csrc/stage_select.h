@@ -30,6 +30,7 @@ struct StageKernels {
     StageFnDeltaTma dx_tma1 = nullptr, dx_tma2 = nullptr; // FP32-mixed increment form
     int tile_x = 0, tile_y = 0, threads = 0; // threads == 0: no such configuration
     size_t smem = 0, smem2 = 0;               // dynamic shared memory per block, stage 1 and 2
+    int halo_w = kTmaHaloW, own_w = kTmaOwnW; // TMA box widths of the increment form's maps
 };
 
 enum StageKernelKind : int {
@@ -37,11 +38,12 @@ enum StageKernelKind : int {
     kKindTileMerged = 1,
     kKindMarch = 2,
     kKindMarchTma = 3,
-    kKindMarchTmaDelta = 4 // TMA strip march of the increment form (stage_delta.cuh)
+    kKindMarchTmaDelta = 4, // TMA strip march of the increment form (stage_delta.cuh)
+    kKindMarchTmaPair = 5   // its two-column form (march_pair.cuh)
 };
 
-// tile_x x tile_y: interior cells one block covers (strip march: warps x 28 columns by the rows
-// of a warp's segment).
+// tile_x x tile_y: interior cells one block covers (strip march: warps x 28 columns, or 60 for
+// the two-column form, by the rows of a warp's segment).
 struct TileConfigInfo {
     int tile_x, tile_y, threads, min_blocks, kind;
 };
@@ -68,7 +70,8 @@ bool encode_march_maps_f64(const double* in, const double* out, const Geometry& 
 // Both stages' tensor maps of the increment form: U^n (18 float planes) and the increment
 // (9 float planes).
 bool encode_march_maps_delta(const MixedState& un, float* delta, const Geometry& g,
-                             MarchTmaMaps* stage1, MarchTmaMaps* stage2, std::string* err);
+                             MarchTmaMaps* stage1, MarchTmaMaps* stage2, std::string* err,
+                             unsigned halo_w = kTmaHaloW, unsigned own_w = kTmaOwnW);
 
 StageKernels select_stage_f64(int limiter, bool nonideal, bool mask, int config);
 StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int config);

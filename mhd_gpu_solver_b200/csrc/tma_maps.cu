@@ -76,15 +76,16 @@ bool encode_march_maps_f64(const double* in, const double* out, const Geometry& 
 }
 
 bool encode_march_maps_delta(const MixedState& un, float* delta, const Geometry& g,
-                             MarchTmaMaps* stage1, MarchTmaMaps* stage2, std::string* err)
+                             MarchTmaMaps* stage1, MarchTmaMaps* stage2, std::string* err,
+                             unsigned halo_w, unsigned own_w)
 {
     *stage1 = MarchTmaMaps{};
     *stage2 = MarchTmaMaps{};
-    return state_tensor_map(un.hi, false, 18, g, kTmaHaloW, 9, &stage1->in_halo, err) &&
-           state_tensor_map(un.hi, false, 18, g, kTmaHaloW, 9, &stage2->in_halo, err) &&
-           state_tensor_map(delta, false, 9, g, kTmaHaloW, 9, &stage2->delta_halo, err) &&
-           state_tensor_map(delta, false, 9, g, kTmaOwnW, 9, &stage2->in_own, err) &&
-           state_tensor_map(un.hi, false, 18, g, kTmaOwnW, 18, &stage2->out_own, err);
+    return state_tensor_map(un.hi, false, 18, g, halo_w, 9, &stage1->in_halo, err) &&
+           state_tensor_map(un.hi, false, 18, g, halo_w, 9, &stage2->in_halo, err) &&
+           state_tensor_map(delta, false, 9, g, halo_w, 9, &stage2->delta_halo, err) &&
+           state_tensor_map(delta, false, 9, g, own_w, 9, &stage2->in_own, err) &&
+           state_tensor_map(un.hi, false, 18, g, own_w, 18, &stage2->out_own, err);
 }
 
 } // namespace mhdb

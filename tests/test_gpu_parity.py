@@ -564,3 +564,35 @@ def test_default_configuration_of_a_large_masked_grid_matches_fp64():
     u32, _, s32, _ = _gpu(U0, orc.Grid(n, n), p, bc, mask, precision=_capi.FP32)
     assert s32 == s64 == 6
     assert_components(u32, u64, MIXED_L1, c64)
+
+
+@pytest.mark.parametrize("case", range(len(MARCH_CASES)))
+@pytest.mark.parametrize("ni", [False, True])
+def test_two_column_strip_march_matches_single_column(case, ni):
+    """The two-column strip march of the increment form (two columns per lane, 60 owned columns
+    per warp) runs the single-column march's arithmetic operand for operand: on partial strips,
+    every boundary rule and every limiter, ideal solves give its values bit for bit, with the same
+    step count and clock; non-ideal ones are held to it and to the FP64 oracle at the FP32-mixed
+    bar. 25 steps: an odd count, so the result ends in the other state buffer."""
+    nx, ny, bcx, bcy, state, lim = MARCH_CASES[case]
+    prim = (wl.fourier_state(nx, ny, 9) if state == "fourier" else wl.four_quadrant(nx, ny, 3))
+    bc = (bcx, bcy)
+    U0 = initial_state(prim, 5.0 / 3.0, bc)
+    kw = NI_PARAMS if ni else {}
+    p = orc.Params(limiter=lim, max_steps=25, fixed_steps=True, **kw)
+    cfgs = _capi.tile_configs(_capi.FP32)
+    pairs = [c["config"] for c in cfgs if c["kind"] == "march_tma_pair"]
+    single = next(c["config"] for c in cfgs if c["kind"] == "march_tma_delta" and c["tile_y"] == 32)
+    assert pairs
+    ref, tr, sr, cr = orc.solve(U0, orc.Grid(nx, ny), p, bc)
+    want, tw, sw, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32, tile_config=single)
+    for cfg in pairs:
+        got, tg, sg, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32, tile_config=cfg)
+        assert sg == sw == sr
+        if not ni:
+            assert tg == tw
+            assert np.array_equal(got, want), (cfg, float(np.max(np.abs(got - want))))
+        else:
+            assert abs(tg - tw) <= 1e-6 * tw
+            assert_components(got, want, MIXED_L1, cr, what=cfg)
+        assert_components(got, ref, MIXED_L1, cr, what=cfg)
