@@ -36,6 +36,7 @@ def _config(precision, kind):
 
 
 @pytest.mark.parametrize("precision,kind", [(_capi.FP32, "march_tma_delta"),
+                                            (_capi.FP32, "march_tma_pair"),
                                             (_capi.FP32, "march_tma"),
                                             (_capi.FP64, "march_tma")])
 def test_single_solve_reports_a_wait_that_ran_out(precision, kind):
