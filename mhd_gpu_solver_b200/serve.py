@@ -3,9 +3,11 @@
 Requests (grid side, initial-state seed and kind, physics parameters, t_end) arrive over time.
 The loop
 
-* admits arrived requests in arrival order while their HBM footprint (two padded FP32-mixed
-  states) fits under the memory cap, generating each initial state directly in HBM (no host
-  state, no upload);
+* admits arrived requests while their HBM footprint (two padded FP32-mixed states) fits under
+  the memory cap, by default the ones of least estimated work first and only while the running
+  requests hold at most a cap of interior cells that still fills the GPU (short requests do not
+  wait for the long ones they would otherwise advance beside), generating each initial state
+  directly in HBM (no host state, no upload);
 * advances every admitted, unfinished request together: each chunk of RK2 steps is one
   persistent launch per stage over all of them, so requests that arrive while others are on the
   GPU join the next chunk (continuous batching);
@@ -58,6 +60,20 @@ class Request:
     @property
     def bc(self):
         return (0, 0) if self.kind == "fourier" else (2, 2)
+
+    def work_estimate(self) -> float:
+        """Zone-updates the request will take, estimated before it runs: cells x t_end / dt with
+        dt the CFL step at a typical signal speed of its state kind (4 for the smooth Fourier
+        states, 7 for the four-quadrant ones), or the non-ideal diffusion limit
+        cfl h^2 / (4 eta_max) where that is smaller (the reference's dt rule, which makes the
+        estimate exact for non-ideal requests)."""
+        h = 1.0 / self.n
+        c_h = 4.0 if self.kind == "fourier" else 7.0
+        dt = 0.4 / (2.0 * c_h * self.n)
+        if self.nonideal:
+            eta = max(NONIDEAL["eta_ohm"], NONIDEAL["eta_hall"], NONIDEAL["eta_ambipolar"])
+            dt = min(dt, 0.4 * h * h / (4.0 * eta))
+        return float(self.n) * self.n * self.t_end / dt
 
 
 @dataclass
@@ -126,9 +142,11 @@ class ServeStats:
     makespan: float = 0.0
     peak_bytes: int = 0
     max_active: int = 0
+    peak_cells: int = 0  # most interior cells admitted and unfinished at once
     chunks: int = 0
     joins: int = 0      # requests admitted while others were on the GPU (continuous batching)
     cap_waits: int = 0  # admission rounds in which the next request waited for memory
+    cell_waits: int = 0  # admission rounds in which the next request waited for the cells cap
     states: dict = field(default_factory=dict)  # rid -> final state when kept
 
     def summary(self) -> dict:
@@ -140,8 +158,10 @@ class ServeStats:
                 "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "peak_hbm_bytes": self.peak_bytes, "max_active": self.max_active,
+                "peak_active_cells": self.peak_cells,
                 "chunks": self.chunks, "joined_mid_flight": self.joins,
-                "admission_waits_for_memory": self.cap_waits}
+                "admission_waits_for_memory": self.cap_waits,
+                "admission_waits_for_cells": self.cell_waits}
 
 
 def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
@@ -160,10 +180,20 @@ def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
 
 def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
           chunk: int = 16, download: bool = True, keep_states: bool = False,
-          tune: bool = True, on_complete=None) -> ServeStats:
+          tune: bool = True, on_complete=None, order: str = "shortest",
+          cells_cap: float = 64e6) -> ServeStats:
     """Serve a request stream in real time with continuous batching. tune: each request runs
     the batch configuration tuned for its size class (see prepare). on_complete(completion,
-    stats) is called after each request finishes (progress records of long streams)."""
+    stats) is called after each request finishes (progress records of long streams).
+
+    Admission: a request is admitted only while the batch's HBM footprint stays under
+    memory_cap. With order="shortest" the arrived requests are admitted by their estimated work
+    (Request.work_estimate, smallest first) and, beyond the memory cap, only while the admitted
+    unfinished requests hold at most cells_cap interior cells (at least one request always runs):
+    64M cells keep the persistent batch kernels as busy as one 8k x 8k grid, and short requests no
+    longer wait for the long ones they would otherwise advance beside step for step. The results
+    do not depend on the order (a solve's values are the same alone and in any mix).
+    order="arrival" admits in arrival order under the memory cap alone."""
     batch = BatchSolver(precision, tune=tune)
     stats = ServeStats()
     results = ResultBuffer()
@@ -172,27 +202,38 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
     active: dict[int, tuple[Request, float]] = {}  # admitted, not finished at the last poll
     done: list = []  # (sid, request, admitted, result, poll time) finished at the last poll
     in_use = 0
+    active_cells = 0
     start = time.perf_counter()
     try:
         while pending or queue or active or done:
             now = time.perf_counter() - start
+            arrived = False
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
-            # admission in arrival order while the footprint fits under the cap
+                arrived = True
+            if arrived and order == "shortest":
+                queue = deque(sorted(queue, key=lambda r: (r.work_estimate(), r.arrival)))
+            # admission while the footprint fits under the caps
             while queue:
                 req = queue[0]
                 need = state_bytes(req.n, req.n)
                 if in_use + need > memory_cap and (active or done):
                     stats.cap_waits += 1
                     break
+                if (order == "shortest" and active
+                        and active_cells + req.n * req.n > cells_cap):
+                    stats.cell_waits += 1
+                    break
                 queue.popleft()
                 if active:
                     stats.joins += 1
                 sid = batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
                 in_use += need
+                active_cells += req.n * req.n
                 active[sid] = (req, time.perf_counter() - start)
             stats.peak_bytes = max(stats.peak_bytes, in_use)
             stats.max_active = max(stats.max_active, len(active))
+            stats.peak_cells = max(stats.peak_cells, active_cells)
             if not active and not done:
                 if pending:
                     time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - start)))
@@ -220,6 +261,7 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
                     r, fin = batch.status(sid)
                     if fin:
                         req, admitted = active.pop(sid)
+                        active_cells -= req.n * req.n
                         done.append((sid, req, admitted, r, polled))
         stats.makespan = time.perf_counter() - start
     finally:

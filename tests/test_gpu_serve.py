@@ -41,3 +41,20 @@ def test_admission_respects_the_memory_cap():
     assert stats.peak_bytes <= cap
     s = stats.summary()
     assert s["p99_ms"] >= s["p50_ms"] > 0.0
+
+
+def test_shortest_first_admission_keeps_results_and_the_cells_cap():
+    """Shortest-estimated-work-first admission under a cap of running cells: every request
+    completes, no admission takes the running cells over the cap (one request always runs), and
+    each result equals the arrival-order serve's bit for bit (a solve's values do not depend on
+    the requests beside it)."""
+    reqs = small_stream(14, seed=11)
+    cap = 2 * max(r.n * r.n for r in reqs)
+    fifo = serve(reqs, keep_states=True, order="arrival")
+    sjf = serve(reqs, keep_states=True, order="shortest", cells_cap=cap)
+    assert len(sjf.completions) == len(fifo.completions) == len(reqs)
+    assert sjf.peak_cells <= cap
+    for req in reqs:
+        assert np.array_equal(sjf.states[req.rid], fifo.states[req.rid]), req
+    steps = {c.rid: c.steps for c in fifo.completions}
+    assert all(c.steps == steps[c.rid] for c in sjf.completions)

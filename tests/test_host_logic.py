@@ -196,3 +196,17 @@ def test_host_rasterize_follows_the_reference_rule_cell_by_cell():
     # the strip's row is row 2 (y = 0.3125); its x range [0.25, 0.35] holds the centre 0.25 but
     # not 0.35000000000000003 (= 0.05 + 3 x 0.1 rounded), so one cell turns fluid
     assert (got == 0).any() and got[2, 2] == 1 and got[2, 3] == 0
+
+
+def test_served_request_work_estimate():
+    """The serving loop's admission order: a non-ideal request's estimate is exact (its dt is
+    the diffusion limit cfl h^2 / (4 eta_max) with eta_max the Hall 1e-2), an ideal one's uses
+    the CFL step at a typical signal speed, and the estimate grows with the grid side."""
+    from mhd_gpu_solver_b200.serve import Request
+
+    ni = Request(rid=0, arrival=0.0, n=512, t_end=0.2, kind="fourier", seed=1, nonideal=True)
+    h = 1.0 / 512
+    assert ni.work_estimate() == pytest.approx(512 * 512 * 0.2 / (0.4 * h * h / 0.04), rel=1e-12)
+    small = Request(rid=1, arrival=0.0, n=128, t_end=0.2, kind="quadrants", seed=1, nonideal=False)
+    big = Request(rid=2, arrival=0.0, n=1024, t_end=0.2, kind="quadrants", seed=1, nonideal=False)
+    assert small.work_estimate() < big.work_estimate() < ni.work_estimate() * 10
