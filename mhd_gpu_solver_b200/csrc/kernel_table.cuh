@@ -46,13 +46,15 @@ struct MarchCfg {
 
 // TMA-fed strip-march configuration: NW warps per block, LY rows per warp, MINB blocks per SM.
 template <int NW_, int LY_, int MINB_, bool HF_ = true, int ST1_ = 1, int ST2_ = 0,
-          bool DELTA_ = false>
+          int DELTA_ = 0>
 struct MarchTmaCfg {
     static constexpr int NW = NW_, LY = LY_, MINB = MINB_;
     static constexpr bool HF = HF_; // wait for the halo row before the x sweep
     static constexpr int ST1 = ST1_; // stage 1: 0 lane stores, 1 or 2 staging slots of TMA stores
     static constexpr int ST2 = ST2_; // the same for stage 2
-    static constexpr bool DELTA = DELTA_; // FP32-mixed increment form (stage_delta.cuh)
+    // FP32-mixed increment form (stage_delta.cuh): 0 no, 1 yes, 2 with stage 2's own-cell delta
+    // taken from the halo stream (MarchTmaLayout kind 2)
+    static constexpr int DELTA = DELTA_;
     static constexpr bool MARCH_TMA = true;
 };
 
@@ -111,16 +113,16 @@ void fill_pair(StageKernels& k)
             k.dx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
                                          PolicyDelta<1>>;
             k.dx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, 0, NI, MASK,
-                                         PolicyDelta<2>>;
+                                         PolicyDelta<2, Cfg::DELTA>>;
         } else {
             k.mx_tma1 = march_tma_kernel<L, 1, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST1, NI, MASK>;
             k.mx_tma2 = march_tma_kernel<L, 2, Cfg::LY, Cfg::NW, Cfg::MINB, Cfg::HF, Cfg::ST2, NI, MASK>;
         }
-        constexpr int K = Cfg::DELTA ? 1 : 0;
+        constexpr int K = Cfg::DELTA;
         k.tile_x = Cfg::NW * kMarchOwned;
         k.tile_y = Cfg::LY;
         k.threads = Cfg::NW * 32;
-        k.smem = march_tma_smem_bytes<1, Cfg::ST1, E, K>(Cfg::NW);
+        k.smem = march_tma_smem_bytes<1, Cfg::ST1, E, (K > 0 ? 1 : 0)>(Cfg::NW);
         k.smem2 = march_tma_smem_bytes<2, Cfg::ST2, E, K>(Cfg::NW);
         return;
     } else if constexpr (is_march<Cfg>::value) {

@@ -17,10 +17,12 @@ using Cfg9 = MarchTmaCfg<1, 32, 16>;
 using Cfg10 = MarchTmaCfg<4, 32, 4, true, 0>;
 using Cfg11 = MarchTmaCfg<1, 32, 16, true, 0>;
 using Cfg12 = MarchTmaCfg<1, 64, 16>;
-using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, true>; // increment form (also masked)
-using Cfg14 = MarchTmaCfg<1, 64, 16, true, 0, 0, true>; // increment form, 64-row segments
+using Cfg13 = MarchTmaCfg<1, 32, 16, true, 0, 0, 1>; // increment form (also masked)
+using Cfg14 = MarchTmaCfg<1, 64, 16, true, 0, 0, 1>; // increment form, 64-row segments
 using Cfg15 = MarchPairCfg<32, 8>;  // increment form, two columns per lane
 using Cfg16 = MarchPairCfg<32, 10>; // the same, 10 blocks per SM requested (168 registers)
+// increment form, stage 2's own-cell delta from the halo stream (also masked)
+using Cfg17 = MarchTmaCfg<1, 32, 16, true, 0, 0, 2>;
 constexpr TileConfigInfo kInfo[] = {
     {32, 16, 256, 2, kKindTile},       {32, 16, 256, 3, kKindTile},
     {32, 8, 256, 3, kKindTile},        {32, 16, 384, 2, kKindTileMerged},
@@ -30,7 +32,7 @@ constexpr TileConfigInfo kInfo[] = {
     {112, 32, 128, 4, kKindMarchTma},  {28, 32, 32, 16, kKindMarchTma},
     {28, 64, 32, 16, kKindMarchTma},   {28, 32, 32, 16, kKindMarchTmaDelta},
     {28, 64, 32, 16, kKindMarchTmaDelta}, {60, 32, 32, 8, kKindMarchTmaPair},
-    {60, 32, 32, 10, kKindMarchTmaPair}};
+    {60, 32, 32, 10, kKindMarchTmaPair}, {28, 32, 32, 16, kKindMarchTmaDelta}};
 constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 } // namespace
 
@@ -82,6 +84,8 @@ StageKernels select_stage_mixed(int limiter, bool nonideal, bool mask, int confi
         return select_unmasked<PolicyMixed, Cfg15>(limiter, nonideal, mask);
     case 16:
         return select_unmasked<PolicyMixed, Cfg16>(limiter, nonideal, mask);
+    case 17:
+        return select_full<PolicyMixed, Cfg17>(limiter, nonideal, mask);
     default:
         return select_full<PolicyMixed, Cfg0>(limiter, nonideal, mask);
     }

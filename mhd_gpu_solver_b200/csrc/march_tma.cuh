@@ -36,9 +36,14 @@ namespace mhdb {
 // box holds 18 hi and lo planes), 8 for the FP64 state (9 planes). KIND 1 is the increment form
 // (stage_delta.cuh): stage 1 has no own stream (its update needs no own-cell operand); stage 2
 // has two halo boxes (hi(U^n), then delta) and own boxes delta (9 planes), then U^n (18).
+// KIND 2 is the increment form whose stage 2 takes the own cells' delta from the halo stream: each
+// owned lane keeps the 9 delta values of its column of the halo row in a 3-row ring of its own
+// (the row is its own row two iterations later), so the own stream copies U^n alone (one box of
+// 18 planes per row instead of two boxes of 27).
 template <int STAGE, int ST, int ELEM = 4, int KIND = 0>
 struct MarchTmaLayout {
-    static constexpr bool kDelta = KIND == 1;
+    static constexpr bool kDelta = KIND >= 1;
+    static constexpr bool kStash = KIND == 2 && STAGE == 2;
     static constexpr int kOwnPlanes = ELEM == 4 ? 18 : 9;
     static constexpr int kHaloBoxBytes = 9 * kTmaHaloW * ELEM;   // 1296 B (FP32), 2592 B (FP64)
     static constexpr int kHaloBoxSlot = (kHaloBoxBytes + 127) / 128 * 128;
@@ -48,16 +53,21 @@ struct MarchTmaLayout {
     static constexpr int kOwnBoxBytes = kOwnPlanes * kTmaOwnW * ELEM; // 2016 B per box
     static constexpr int kOwnBoxSlot = (kOwnBoxBytes + 127) / 128 * 128; // 2048 B
     // own box A (the stage input's own cells; delta in the increment form) and box B (U^n)
-    static constexpr int kOwnPlanesA = kDelta ? 9 : kOwnPlanes;
+    static constexpr int kOwnPlanesA = kStash ? 0 : (kDelta ? 9 : kOwnPlanes);
     static constexpr int kOwnABytes = kOwnPlanesA * kTmaOwnW * ELEM;
     static constexpr int kOwnBOff = (kOwnABytes + 127) / 128 * 128; // byte offset of box B
-    static constexpr int kOwnBoxes = kDelta ? (STAGE == 1 ? 0 : 2) : (STAGE == 1 ? 1 : 2);
+    static constexpr int kOwnBoxes =
+        kStash ? 1 : (kDelta ? (STAGE == 1 ? 0 : 2) : (STAGE == 1 ? 1 : 2));
     static constexpr int kOwnSlot = kOwnBoxes == 0 ? 0 : (kOwnBoxes == 1 ? kOwnBoxSlot
                                                                         : kOwnBOff + kOwnBoxSlot);
     static constexpr int kOwnTx = kOwnBoxes == 0 ? 0 : (kOwnBoxes == 1 ? kOwnBoxBytes
                                                                       : kOwnABytes + kOwnBoxBytes);
     static constexpr int kStageOff = 2 * kHaloSlot + 2 * kOwnSlot;
-    static constexpr int kBarOff = kStageOff + ST * kOwnBoxSlot;
+    // delta ring (kStash): 3 rows x 9 planes x the owned columns
+    static constexpr int kStashRow = 9 * kTmaOwnW;
+    static constexpr int kStashOff = kStageOff + ST * kOwnBoxSlot;
+    static constexpr int kStashBytes = kStash ? (3 * kStashRow * 4 + 127) / 128 * 128 : 0;
+    static constexpr int kBarOff = kStashOff + kStashBytes;
     static constexpr int kWarpBytes = kBarOff + 128;             // 4 mbarriers, padded
 };
 
@@ -73,7 +83,8 @@ constexpr bool fits_16_blocks(size_t bytes) { return 16 * (bytes + 1024) <= 228 
 static_assert(fits_16_blocks(march_tma_smem_bytes<1, 1>(1)) &&
                   fits_16_blocks(march_tma_smem_bytes<2, 0>(1)) &&
                   fits_16_blocks(march_tma_smem_bytes<1, 0, 4, 1>(1)) &&
-                  fits_16_blocks(march_tma_smem_bytes<2, 0, 4, 1>(1)),
+                  fits_16_blocks(march_tma_smem_bytes<2, 0, 4, 1>(1)) &&
+                  fits_16_blocks(march_tma_smem_bytes<2, 0, 4, 2>(1)),
               "a one-warp FP32-mixed strip-march layout no longer fits 16 blocks per SM");
 
 template <int L, int STAGE, int LY, bool HF, int ST, bool NI, bool MASK = false,
@@ -110,6 +121,8 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
     const T* halo_f = reinterpret_cast<const T*>(wbase);
     const T* own_f = reinterpret_cast<const T*>(wbase + 2 * Lay::kHaloSlot);
     float* stg_f = reinterpret_cast<float*>(wbase + Lay::kStageOff);
+    // delta ring (kStash): row item j in slot j % 3, this lane's owned column at lane - 2
+    float* stash_f = reinterpret_cast<float*>(wbase + Lay::kStashOff) + (lane >= 2 ? lane - 2 : 0);
     const uint32_t halo_s = smem_addr(wbase);
     const uint32_t own_s = halo_s + 2 * Lay::kHaloSlot;
     const uint32_t stg_s = halo_s + Lay::kStageOff;
@@ -146,7 +159,9 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             const uint32_t bar = bar_s + 16 + 8 * slot;
             const uint32_t dst = own_s + slot * Lay::kOwnSlot;
             mbar_arrive_expect_tx(bar, Lay::kOwnTx);
-            tma_load_3d(dst, &m.in_own, bar, x0, y0 + i, 0);
+            if constexpr (Lay::kOwnPlanesA > 0) {
+                tma_load_3d(dst, &m.in_own, bar, x0, y0 + i, 0);
+            }
             if constexpr (STAGE == 2) {
                 tma_load_3d(dst + Lay::kOwnBOff, &m.out_own, bar, x0, y0 + i, 0);
             }
@@ -258,6 +273,22 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             sYc[c] = limit_half_slope<L>(Wm[c] - wb[c], Wp[c] - Wm[c]);
         }
         face_flux_regs<T, true, true>(wb, sYm, Wm, sYc, gamma, inv_gm1, c_h, Gm);
+        if constexpr (Lay::kStash) {
+            // the own cells' delta of rows y0 and y0 + 1 (the ring's first two items)
+            if (own) {
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                    if (r < nrows) {
+                        const size_t o = static_cast<size_t>(y0 + r) * g.pitch + gx;
+#pragma unroll
+                        for (int c = 0; c < 9; ++c) {
+                            stash_f[r * Lay::kStashRow + c * kTmaOwnW] =
+                                __ldg(a.delta + static_cast<size_t>(c) * g.plane + o);
+                        }
+                    }
+                }
+            }
+        }
         if constexpr (NI) {
             T Jb[3];
             march_current(wa, wb, Wm, inv_2dx, inv_2dy, Jb);
@@ -268,6 +299,7 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
 
     double smax = 0.0;
     bool failed = false;
+    int ring_rd = 0, ring_wr = 2; // delta ring slots of rows y and y + 2 (kStash)
 #pragma unroll 1
     for (int i = 0; i < nrows; ++i) {
         const int y = y0 + i;
@@ -314,8 +346,13 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
                 for (int c = 0; c < 9; ++c) {
                     rn.v[c] = src[c * kTmaHaloW];
                     if constexpr (Lay::kHaloBoxes == 2) { // U* hi = fl(hi(U^n) + delta)
-                        rn.v[c] = __fadd_rn(rn.v[c],
-                                            src[Lay::kHaloBoxSlot / sizeof(T) + c * kTmaHaloW]);
+                        const T dl = src[Lay::kHaloBoxSlot / sizeof(T) + c * kTmaHaloW];
+                        if constexpr (Lay::kStash) {
+                            if (own && i + 2 < nrows) {
+                                stash_f[ring_wr * Lay::kStashRow + c * kTmaOwnW] = dl;
+                            }
+                        }
+                        rn.v[c] = __fadd_rn(rn.v[c], dl);
                     }
                 }
             } else {
@@ -366,6 +403,10 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             // own-cell operand q: plane q of box A (the stage input; delta in the increment
             // form), then (stage 2) plane q - kOwnPlanesA of box B (U^n)
             auto op = [&](int q) {
+                if constexpr (Lay::kStash) { // delta from the ring, U^n from box B
+                    return q < 9 ? stash_f[ring_rd * Lay::kStashRow + q * kTmaOwnW]
+                                 : src[(q - 9) * kTmaOwnW];
+                }
                 return q < Lay::kOwnPlanesA
                            ? src[q * kTmaOwnW]
                            : src[Lay::kOwnBOff / sizeof(T) + (q - Lay::kOwnPlanesA) * kTmaOwnW];
@@ -481,6 +522,10 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
             if (i + 2 < nrows && Lay::kOwnBoxes > 0) {
                 own_issued = i + 3;
             }
+        }
+        if constexpr (Lay::kStash) {
+            ring_rd = ring_rd == 2 ? 0 : ring_rd + 1;
+            ring_wr = ring_wr == 2 ? 0 : ring_wr + 1;
         }
 #pragma unroll
         for (int c = 0; c < 9; ++c) {

@@ -33,11 +33,13 @@ struct StageArgsDelta {
     int walls;
 };
 
-template <int STAGE>
+// LAYOUT: MarchTmaLayout kind of the TMA strip march (1: own cells' delta through the own
+// stream; 2: through the halo stream, kept in a ring per lane).
+template <int STAGE, int LAYOUT = 1>
 struct PolicyDelta {
     using T = float;
     using Args = StageArgsDelta;
-    static constexpr int kLayout = 1; // MarchTmaLayout of the increment form
+    static constexpr int kLayout = LAYOUT;
     struct Raw {
         float v[9];
     };

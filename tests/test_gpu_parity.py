@@ -596,3 +596,58 @@ def test_two_column_strip_march_matches_single_column(case, ni):
             assert abs(tg - tw) <= 1e-6 * tw
             assert_components(got, want, MIXED_L1, cr, what=cfg)
         assert_components(got, ref, MIXED_L1, cr, what=cfg)
+
+
+def _config_of(precision, kind, **shape):
+    return [c["config"] for c in _capi.tile_configs(precision) if c["kind"] == kind
+            and all(c[k] == v for k, v in shape.items())]
+
+
+@pytest.mark.parametrize("case", range(len(MARCH_CASES)))
+@pytest.mark.parametrize("ni", [False, True])
+def test_increment_form_delta_ring_matches_own_stream(case, ni):
+    """Stage 2 of the increment form with the own cells' delta taken from the halo stream (kept
+    in a 3-row ring per lane) against the same march reading it through the own stream: the same
+    operands, so ideal solves agree bit for bit (same step count and clock); non-ideal ones are
+    held to it at the FP32-mixed bar, and both to the FP64 oracle. 25 steps (odd: the result ends
+    in the other state buffer); partial strips and segments, every boundary rule and limiter."""
+    nx, ny, bcx, bcy, state, lim = MARCH_CASES[case]
+    prim = (wl.fourier_state(nx, ny, 9) if state == "fourier" else wl.four_quadrant(nx, ny, 3))
+    bc = (bcx, bcy)
+    U0 = initial_state(prim, 5.0 / 3.0, bc)
+    kw = NI_PARAMS if ni else {}
+    p = orc.Params(limiter=lim, max_steps=25, fixed_steps=True, **kw)
+    delta = _config_of(_capi.FP32, "march_tma_delta", tile_y=32, min_blocks=16)
+    assert len(delta) >= 2
+    ref, tr, sr, cr = orc.solve(U0, orc.Grid(nx, ny), p, bc)
+    want, tw, sw, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32,
+                           tile_config=delta[0])
+    for cfg in delta[1:]:
+        got, tg, sg, _ = _gpu(U0, orc.Grid(nx, ny), p, bc, precision=_capi.FP32, tile_config=cfg)
+        assert sg == sw == sr
+        if not ni:
+            assert tg == tw
+            assert np.array_equal(got, want), (cfg, float(np.max(np.abs(got - want))))
+        else:
+            assert abs(tg - tw) <= 1e-6 * tw
+            assert_components(got, want, MIXED_L1, cr, what=cfg)
+        assert_components(got, ref, MIXED_L1, cr, what=cfg)
+
+
+@pytest.mark.parametrize("walls", [True, False])
+def test_masked_increment_form_delta_ring_matches_own_stream(walls):
+    """The same with solid cells on every edge (their stage-2 update reads the delta ring too):
+    bit for bit against the own-stream march, within the FP32-mixed bar of the FP64 oracle."""
+    nx, ny = 61, 45
+    bc = (orc.OUTFLOW, orc.PERIODIC)
+    mask = _edge_mask(nx, ny, seed=11)
+    U0 = initial_state(wl.fourier_state(nx, ny, 6), 5.0 / 3.0, bc, mask, walls)
+    p = orc.Params(limiter=orc.VANLEER, max_steps=25, fixed_steps=True)
+    ref, tr, sr, cr = orc.solve(U0, orc.Grid(nx, ny), p, bc, mask, walls)
+    delta = _config_of(_capi.FP32, "march_tma_delta", tile_y=32, min_blocks=16)
+    outs = [_gpu(U0, orc.Grid(nx, ny), p, bc, mask, walls, precision=_capi.FP32, tile_config=c)
+            for c in delta]
+    for got, tg, sg, _ in outs:
+        assert sg == sr and tg == outs[0][1]
+        assert np.array_equal(got, outs[0][0])
+        assert_components(got, ref, MIXED_L1, cr)
