@@ -254,7 +254,7 @@ struct BatchKernels<PolicyMixed> {
         if (v == 1) return 0;
         if (v == 3) {
             return stage == 1 ? march_tma_smem_bytes<1, 0, 4, 1>(1)
-                              : march_tma_smem_bytes<2, 0, 4, 1>(1);
+                              : march_tma_smem_bytes<2, 0, 4, 2>(1);
         }
         return stage == 1 ? march_tma_smem_bytes<1, 1>(1) : march_tma_smem_bytes<2, 0>(1);
     }

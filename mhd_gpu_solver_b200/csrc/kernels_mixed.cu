@@ -39,12 +39,13 @@ constexpr int kCount = sizeof(kInfo) / sizeof(kInfo[0]);
 int stage_config_count_mixed() { return kCount; }
 
 // Without a chosen configuration: grids of at least 1024^2 cells run the TMA strip march with one
-// warp per block, unmasked ones in the increment form (configuration 13), masked ones in the
-// stored form that also serves masks (configuration 11); smaller grids have too few 28-column
-// strips to fill the GPU with it and run the shared-memory tile kernel.
+// warp per block, unmasked ones in the increment form with stage 2's own-cell increment taken
+// from the halo stream (configuration 17), masked ones in the stored form that also serves masks
+// (configuration 11); smaller grids have too few 28-column strips to fill the GPU with it and run
+// the shared-memory tile kernel.
 int default_stage_config_mixed(long long cells, bool mask)
 {
-    return cells >= 1024LL * 1024 ? (mask ? 11 : 13) : 0;
+    return cells >= 1024LL * 1024 ? (mask ? 11 : 17) : 0;
 }
 
 TileConfigInfo stage_config_info_mixed(int c) { return kInfo[c < 0 || c >= kCount ? 0 : c]; }

@@ -687,7 +687,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) batch_march_delta_kernel(
     extern __shared__ unsigned char march_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base = march_smem + ((128u - (smem_addr(march_smem) & 127u)) & 127u);
-    unsigned char* wbase = base + warp * MarchTmaLayout<STAGE, 0, 4, 1>::kWarpBytes;
+    unsigned char* wbase = base + warp * MarchTmaLayout<STAGE, 0, 4, 2>::kWarpBytes;
     bool failed = false;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int2 it = work[w];
@@ -728,7 +728,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) batch_march_delta_kernel(
                 }
             }
             __syncwarp();
-            smax = march_tma_strip<L, STAGE, LY, HF, 0, NI, false, PolicyDelta<STAGE>>(
+            smax = march_tma_strip<L, STAGE, LY, HF, 0, NI, false, PolicyDelta<STAGE, 2>>(
                 sa, m, x0, y0, lane, wbase, failed);
         }
         if constexpr (STAGE == 2) {
