@@ -136,7 +136,7 @@ def test_bench_traffic_lookup_covers_every_march_tma_kind():
     kind: both TMA strip-march forms have one, scaled by cells; other kinds report none."""
     import bench
 
-    for kind, s2 in (("march_tma", 215.1), ("march_tma_delta", 186.4)):
+    for kind, s2 in (("march_tma", 215.1), ("march_tma_delta", 182.9)):
         traffic, src = bench.measured_traffic(kind, 2, 1000.0)
         assert traffic == pytest.approx(s2 * 1000.0) and src
     assert bench.measured_traffic("tile", 2, 1000.0) == (None, None)
