@@ -178,8 +178,8 @@ long long mhdb_launch_count(const mhdb_solver* h);
 
 /* Additive: tile configurations of the stage kernels. Configuration 0 (the shared-memory tile
    kernel) serves every solve; the others serve solves without a mask (the strip-march ones ideal
-   and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configurations 11 and
-   13 and FP64 configuration 7 also masked solves; a solve they do not serve runs the default of its size, see below) and are
+   and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configurations 11,
+   13 and 17 and FP64 configuration 7 also masked solves; a solve they do not serve runs the default of its size, see below) and are
    picked per grid size class by the autotuner
    (mhd_gpu_solver_b200.autotune). mhdb_tile_config_info writes the interior cells one CTA covers
    (tile width and height), threads per CTA and the minimum CTAs per SM of one configuration;
@@ -187,7 +187,8 @@ long long mhdb_launch_count(const mhdb_solver* h);
    y sweeps), MHDB_KERNEL_TILE_MERGED (merged sweeps), MHDB_KERNEL_MARCH (warp strip march, 28
    columns per warp), MHDB_KERNEL_MARCH_TMA (the strip march fed by TMA bulk copies into shared
    memory), MHDB_KERNEL_MARCH_TMA_DELTA (the same for the FP32-mixed increment form: stage 1
-   stores the FP32 increment dt L instead of U*, stage 2 reads U^n + increment) or
+   stores the FP32 increment dt L instead of U*, stage 2 reads U^n + increment; configuration 17
+   takes stage 2's own-cell increment from its halo copies) or
    MHDB_KERNEL_MARCH_TMA_PAIR (the increment form with two columns per lane, 60 columns per warp),
    or -1 for an unknown configuration. */
 enum { MHDB_KERNEL_TILE = 0, MHDB_KERNEL_TILE_MERGED = 1, MHDB_KERNEL_MARCH = 2,

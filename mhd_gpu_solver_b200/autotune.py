@@ -6,9 +6,9 @@ to a power of two, per precision form and limiter) the tuner times each configur
 synthetic smooth state for a few RK2 steps, with CUDA events on the solver's stream, and
 remembers the fastest. Results are cached in memory for the process and can be saved to / loaded
 from a JSON file. Configurations other than 0 serve unmasked solves (the strip-march ones ideal
-and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configurations 11 and
-13 and FP64 configuration 7 also masked solves); a solve that the chosen configuration does not serve runs the library's default
-for its size.
+and non-ideal solves, the other tile ones ideal solves only; FP32-mixed configurations 11, 13
+and 17 and FP64 configuration 7 also masked solves); a solve that the chosen configuration does
+not serve runs the library's default for its size.
 
 ``tune_batch`` does the same for the batched form: per (precision, limiter, ideal or non-ideal,
 size class) it times every batch configuration (``batch.batch_configs``: strip march with or

@@ -267,10 +267,16 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
         prim(y0 - 1, r1, wb);
         prim(y0, r2, Wm);
         prim(y0 + 1, r3, Wp);
+        {
+            T d0[9], d1[9], d2[9];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            sYm[c] = limit_half_slope<L>(wb[c] - wa[c], Wm[c] - wb[c]);
-            sYc[c] = limit_half_slope<L>(Wm[c] - wb[c], Wp[c] - Wm[c]);
+            for (int c = 0; c < 9; ++c) {
+                d0[c] = wb[c] - wa[c];
+                d1[c] = Wm[c] - wb[c];
+                d2[c] = Wp[c] - Wm[c];
+            }
+            limit_half_slopes<L>(d0, d1, sYm);
+            limit_half_slopes<L>(d1, d2, sYc);
         }
         face_flux_regs<T, true, true>(wb, sYm, Wm, sYc, gamma, inv_gm1, c_h, Gm);
         if constexpr (Lay::kStash) {
@@ -307,12 +313,15 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
         T dF[9];
         auto x_sweep = [&]() {
             T Wn[9], sX[9], sXn[9], F[9];
+            {
+                T dL[9], dR[9];
 #pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                Wn[c] = __shfl_down_sync(kFull, Wm[c], 1);
-                const T dR = Wn[c] - Wm[c];
-                const T dL = __shfl_up_sync(kFull, dR, 1);
-                sX[c] = limit_half_slope<L>(dL, dR);
+                for (int c = 0; c < 9; ++c) {
+                    Wn[c] = __shfl_down_sync(kFull, Wm[c], 1);
+                    dR[c] = Wn[c] - Wm[c];
+                    dL[c] = __shfl_up_sync(kFull, dR[c], 1);
+                }
+                limit_half_slopes<L>(dL, dR, sX);
             }
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
@@ -371,9 +380,14 @@ __device__ __forceinline__ double march_tma_strip(const typename Policy::Args& a
         if constexpr (HF) {
             x_sweep(); // after the halo wait: the x and y fluxes share one scheduling region
         }
+        {
+            T dm[9], dp[9];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            sYn[c] = limit_half_slope<L>(Wp[c] - Wm[c], W2[c] - Wp[c]);
+            for (int c = 0; c < 9; ++c) {
+                dm[c] = Wp[c] - Wm[c];
+                dp[c] = W2[c] - Wp[c];
+            }
+            limit_half_slopes<L>(dm, dp, sYn);
         }
         face_flux_regs<T, true, true>(Wm, sYc, Wp, sYn, gamma, inv_gm1, c_h, Gp);
         T Jn[NI ? 3 : 1];

@@ -153,6 +153,47 @@ __device__ __forceinline__ T limit_half_slope(T a, T b)
     }
 }
 
+// limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division per pair of
+// components (the simultaneous-inversion identity 1/s1 = s2 / (s1 s2), 1/s2 = s1 / (s1 s2), with
+// s = a + b where ab > 0 and 1 where the slope is 0 anyway): 5 divisions instead of 9, each
+// reciprocal within 2 ulp of 1/s. A pair whose product leaves the normal range takes its two
+// divisions separately. Every other limiter and precision: component by component.
+template <int L, class T>
+__device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[9], T (&out)[9])
+{
+    if constexpr (L == kVanLeer && sizeof(T) == 8) {
+        T p[9], s[9], r[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            p[c] = a[c] * b[c];
+            s[c] = (p[c] > T(0)) ? a[c] + b[c] : T(1);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; c += 2) {
+            const T prod = s[c] * s[c + 1];
+            const T mag = fabs(prod);
+            if (mag >= 2.2250738585072014e-308 && mag <= 1.7976931348623157e308) {
+                const T inv = T(1) / prod;
+                r[c] = s[c + 1] * inv;
+                r[c + 1] = s[c] * inv;
+            } else {
+                r[c] = T(1) / s[c];
+                r[c + 1] = T(1) / s[c + 1];
+            }
+        }
+        r[8] = T(1) / s[8];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            out[c] = (p[c] <= T(0)) ? T(0) : p[c] * r[c];
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            out[c] = limit_half_slope<L>(a[c], b[c]);
+        }
+    }
+}
+
 // Face i-1/2 from cells (i-2, i-1, i, i+1); include/mhd/kernels/muscl_hll.hpp:59-68.
 template <int L, class T>
 __device__ __forceinline__ void reconstruct(T wmm, T wm, T w0, T wp, T& left, T& right)

@@ -378,8 +378,8 @@ StepPlan make_plan(mhdb_solver* h, const mhdb_params* p)
     const bool ni = s.k.ni_any != 0;
     StageKernels sk{};
     // Configurations other than 0 serve unmasked solves (the tile ones ideal solves only, the
-    // strip-march ones non-ideal solves too; FP32-mixed configurations 11 and 13 and FP64
-    // configuration 7 also masked solves). A
+    // strip-march ones non-ideal solves too; FP32-mixed configurations 11, 13 and 17 and
+    // FP64 configuration 7 also masked solves). A
     // solve the chosen configuration does not serve (e.g. a masked solve after an autotuner
     // choice made on unmasked grids) uses the default configuration of its size, else 0.
     const long long cells = static_cast<long long>(h->grid.nx) * h->grid.ny;
