@@ -153,11 +153,11 @@ __device__ __forceinline__ T limit_half_slope(T a, T b)
     }
 }
 
-// limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division per pair of
-// components (the simultaneous-inversion identity 1/s1 = s2 / (s1 s2), 1/s2 = s1 / (s1 s2), with
-// s = a + b where ab > 0 and 1 where the slope is 0 anyway): 5 divisions instead of 9, each
-// reciprocal within 2 ulp of 1/s. A pair whose product leaves the normal range takes its two
-// divisions separately. Every other limiter and precision: component by component.
+// limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division per three
+// components (simultaneous inversion: with q = 1 / (s0 s1 s2), 1/s2 = (s0 s1) q, 1/s0 = s1 (s2 q),
+// 1/s1 = s0 (s2 q), where s = a + b if ab > 0 and 1 where the slope is 0 anyway): 3 divisions
+// instead of 9, each reciprocal within 3 ulp of 1/s. A group whose product leaves the normal range
+// takes its divisions separately. Every other limiter and precision: component by component.
 template <int L, class T>
 __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[9], T (&out)[9])
 {
@@ -169,19 +169,22 @@ __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[
             s[c] = (p[c] > T(0)) ? a[c] + b[c] : T(1);
         }
 #pragma unroll
-        for (int c = 0; c < 8; c += 2) {
-            const T prod = s[c] * s[c + 1];
+        for (int c = 0; c < 9; c += 3) {
+            const T p01 = s[c] * s[c + 1];
+            const T prod = p01 * s[c + 2];
             const T mag = fabs(prod);
             if (mag >= 2.2250738585072014e-308 && mag <= 1.7976931348623157e308) {
                 const T inv = T(1) / prod;
-                r[c] = s[c + 1] * inv;
-                r[c + 1] = s[c] * inv;
+                r[c + 2] = p01 * inv;
+                const T inv01 = s[c + 2] * inv;
+                r[c] = s[c + 1] * inv01;
+                r[c + 1] = s[c] * inv01;
             } else {
                 r[c] = T(1) / s[c];
                 r[c + 1] = T(1) / s[c + 1];
+                r[c + 2] = T(1) / s[c + 2];
             }
         }
-        r[8] = T(1) / s[8];
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
             out[c] = (p[c] <= T(0)) ? T(0) : p[c] * r[c];
