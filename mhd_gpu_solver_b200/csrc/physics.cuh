@@ -153,11 +153,12 @@ __device__ __forceinline__ T limit_half_slope(T a, T b)
     }
 }
 
-// limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division per three
-// components (simultaneous inversion: with q = 1 / (s0 s1 s2), 1/s2 = (s0 s1) q, 1/s0 = s1 (s2 q),
-// 1/s1 = s0 (s2 q), where s = a + b if ab > 0 and 1 where the slope is 0 anyway): 3 divisions
-// instead of 9, each reciprocal within 3 ulp of 1/s. A group whose product leaves the normal range
-// takes its divisions separately. Every other limiter and precision: component by component.
+// limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division for all
+// nine (simultaneous inversion over a two-level product tree: groups g_j = s_3j s_3j+1 s_3j+2,
+// q = 1 / (g_0 g_1 g_2), 1/g_2 = (g_0 g_1) q, 1/g_0 = g_1 (g_2 q), 1/g_1 = g_0 (g_2 q), then the
+// same within each group; s = a + b if ab > 0 and 1 where the slope is 0 anyway), each reciprocal
+// within 6 ulp of 1/s. If the product leaves the normal range, every component takes its own
+// division. Every other limiter and precision: component by component.
 template <int L, class T>
 __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[9], T (&out)[9])
 {
@@ -168,21 +169,33 @@ __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[
             p[c] = a[c] * b[c];
             s[c] = (p[c] > T(0)) ? a[c] + b[c] : T(1);
         }
+        T p01[3], g[3];
 #pragma unroll
-        for (int c = 0; c < 9; c += 3) {
-            const T p01 = s[c] * s[c + 1];
-            const T prod = p01 * s[c + 2];
-            const T mag = fabs(prod);
-            if (mag >= 2.2250738585072014e-308 && mag <= 1.7976931348623157e308) {
-                const T inv = T(1) / prod;
-                r[c + 2] = p01 * inv;
-                const T inv01 = s[c + 2] * inv;
-                r[c] = s[c + 1] * inv01;
-                r[c + 1] = s[c] * inv01;
-            } else {
+        for (int j = 0; j < 3; ++j) {
+            p01[j] = s[3 * j] * s[3 * j + 1];
+            g[j] = p01[j] * s[3 * j + 2];
+        }
+        const T g01 = g[0] * g[1];
+        const T prod = g01 * g[2];
+        const T mag = fabs(prod);
+        if (mag >= 2.2250738585072014e-308 && mag <= 1.7976931348623157e308) {
+            const T inv = T(1) / prod;
+            T ig[3];
+            ig[2] = g01 * inv;
+            const T i01 = g[2] * inv;
+            ig[0] = g[1] * i01;
+            ig[1] = g[0] * i01;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                r[3 * j + 2] = p01[j] * ig[j];
+                const T t = s[3 * j + 2] * ig[j];
+                r[3 * j] = s[3 * j + 1] * t;
+                r[3 * j + 1] = s[3 * j] * t;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
                 r[c] = T(1) / s[c];
-                r[c + 1] = T(1) / s[c + 1];
-                r[c + 2] = T(1) / s[c + 2];
             }
         }
 #pragma unroll
