@@ -153,12 +153,26 @@ __device__ __forceinline__ T limit_half_slope(T a, T b)
     }
 }
 
+// 1/x for a normal or infinite FP64 x without a division: the hardware approximation
+// rcp.approx.ftz.f64 refined by two Newton-Raphson steps e = 1 - x y, y += y e (the classical
+// iteration, each step squaring the relative error), so within a few ulp of 1/x; 0 for |x| of
+// 2^1022 and above. Used only where a product of slopes left the normal range.
+__device__ __forceinline__ double newton_rcp(double x)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
 // limit_half_slope of nine components (a[c], b[c]). FP64 van Leer takes one division for all
 // nine (simultaneous inversion over a two-level product tree: groups g_j = s_3j s_3j+1 s_3j+2,
 // q = 1 / (g_0 g_1 g_2), 1/g_2 = (g_0 g_1) q, 1/g_0 = g_1 (g_2 q), 1/g_1 = g_0 (g_2 q), then the
 // same within each group; s = a + b if ab > 0 and 1 where the slope is 0 anyway), each reciprocal
 // within 6 ulp of 1/s. If the product leaves the normal range, every component takes its own
-// division. Every other limiter and precision: component by component.
+// reciprocal (newton_rcp). Every other limiter and precision: component by component.
 template <int L, class T>
 __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[9], T (&out)[9])
 {
@@ -195,7 +209,7 @@ __device__ __forceinline__ void limit_half_slopes(const T (&a)[9], const T (&b)[
         } else {
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
-                r[c] = T(1) / s[c];
+                r[c] = newton_rcp(s[c]);
             }
         }
 #pragma unroll
@@ -222,9 +236,8 @@ __device__ __forceinline__ void reconstruct(T wmm, T wm, T w0, T wp, T& left, T&
 
 // Fast magnetosonic speed along n; include/mhd/kernels/muscl_hll.hpp:70-87.
 template <class T>
-__device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
+__device__ __forceinline__ T fast_speed_n_inv(const PrimN<T>& W, T inv_rho, T gamma)
 {
-    const T inv_rho = fast_rcp(W.rho);
     const T cs2 = gamma * W.p * inv_rho;
     const T bn2 = W.bn * W.bn;
     const T b2 = bn2 + W.bt * W.bt + W.bz * W.bz;
@@ -234,6 +247,11 @@ __device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
     const T disc = vmax(sum * sum - T(4) * cs2 * van2, T(0));
     const T cf2 = T(0.5) * (sum + fast_sqrt(disc));
     return fast_sqrt(vmax(cf2, T(0)));
+}
+template <class T>
+__device__ __forceinline__ T fast_speed_n(const PrimN<T>& W, T gamma)
+{
+    return fast_speed_n_inv(W, fast_rcp(W.rho), gamma);
 }
 
 // Conserved state and GLM-MHD flux along n; include/mhd/kernels/muscl_hll.hpp:89-124.
@@ -357,13 +375,13 @@ __device__ __forceinline__ T cell_max_signal_speed(T rho, T mx, T my, T mz, T en
     W.bt = by;
     W.bz = bz;
     W.psi = T(0);
-    const T sx = fabs(W.vn) + fast_speed_n(W, gamma);
+    const T sx = fabs(W.vn) + fast_speed_n_inv(W, inv_rho, gamma);
     PrimN<T> Wy = W;
     Wy.vn = W.vt;
     Wy.vt = W.vn;
     Wy.bn = by;
     Wy.bt = bx;
-    const T sy = fabs(Wy.vn) + fast_speed_n(Wy, gamma);
+    const T sy = fabs(Wy.vn) + fast_speed_n_inv(Wy, inv_rho, gamma);
     return vmax(sx, sy);
 }
 
