@@ -71,11 +71,29 @@ __device__ __forceinline__ void slope_item(const T* __restrict__ sW, T* __restri
     constexpr int step = YDIR ? HX : 1;
     const int sx = t % W, sy = t / W;
     const int i = YDIR ? (sy + 1) * HX + (sx + 2) : (sy + 2) * HX + (sx + 1);
+    if constexpr (L == kVanLeer && sizeof(T) == 8) {
+        // the nine components at once: one division (limit_half_slopes), slope = 2 x half
+        // slope (exact)
+        T dm[9], dp[9], h[9];
 #pragma unroll
-    for (int c = 0; c < 9; ++c) {
-        const T* w = sW + c * S::NH + i;
-        const T wm = w[-step], w0 = w[0], wp = w[step];
-        sS[c * sn + t] = limit_slope<L>(w0 - wm, wp - w0);
+        for (int c = 0; c < 9; ++c) {
+            const T* w = sW + c * S::NH + i;
+            const T wm = w[-step], w0 = w[0], wp = w[step];
+            dm[c] = w0 - wm;
+            dp[c] = wp - w0;
+        }
+        limit_half_slopes<L>(dm, dp, h);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            sS[c * sn + t] = T(2) * h[c];
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const T* w = sW + c * S::NH + i;
+            const T wm = w[-step], w0 = w[0], wp = w[step];
+            sS[c * sn + t] = limit_slope<L>(w0 - wm, wp - w0);
+        }
     }
 }
 
