@@ -14,8 +14,10 @@ The loop
 * when a request finishes, downloads its result while the next chunk runs, frees its memory and
   records its latency (completion minus arrival).
 
-``serve_one_at_a_time`` runs the same requests through the plain FP64 single-solve path, one after
-the other, as the comparison. ``make_stream`` draws a seeded request stream: Poisson arrivals,
+``serve`` replays a request stream with given arrival times; ``Server`` is the online form (a
+worker thread runs the same engine while requests are submitted from any thread, with
+submit/poll/result/summary). ``serve_one_at_a_time`` runs the same requests through the plain
+FP64 single-solve path, one after the other, as the comparison. ``make_stream`` draws a seeded request stream: Poisson arrivals,
 side log-uniform, t_end uniform, Fourier or four-quadrant states 50/50, and a fraction with
 Ohmic, Hall and ambipolar terms.
 """
@@ -23,6 +25,7 @@ Ohmic, Hall and ambipolar terms.
 from __future__ import annotations
 
 import math
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -178,6 +181,104 @@ def prepare(requests: list[Request], precision: int = _capi.FP32) -> None:
             autotune.tune_batch(precision, req.limiter, req.n, req.n, ni)
 
 
+class _Engine:
+    """The continuous-batching core shared by serve() and Server: admission under the memory
+    and cells caps, chunked advance of every admitted request, completion of finished ones. All
+    of its calls come from one thread."""
+
+    def __init__(self, precision: int, memory_cap: float, chunk: int, download: bool,
+                 keep_states: bool, tune: bool, order: str, cells_cap: float, stats: ServeStats,
+                 on_complete=None, start: float | None = None):
+        if order not in ("shortest", "arrival"):
+            raise ValueError(f"unknown admission order {order!r}")
+        self.batch = BatchSolver(precision, tune=tune)
+        self.results = ResultBuffer()
+        self.memory_cap, self.chunk, self.download = memory_cap, chunk, download
+        self.keep_states, self.order, self.cells_cap = keep_states, order, cells_cap
+        self.stats = stats
+        self.on_complete = on_complete
+        self.active: dict[int, tuple[Request, float]] = {}  # admitted, not finished at last poll
+        self.done: list = []  # (sid, request, admitted, result, poll time) finished at last poll
+        self.in_use = 0
+        self.active_cells = 0
+        self.start = time.perf_counter() if start is None else start  # the clock's origin
+
+    def clock(self) -> float:
+        return time.perf_counter() - self.start
+
+    @property
+    def busy(self) -> bool:
+        return bool(self.active or self.done)
+
+    def order_queue(self, queue: deque) -> deque:
+        if self.order == "shortest":
+            return deque(sorted(queue, key=lambda r: (r.work_estimate(), r.arrival)))
+        return queue
+
+    def admit(self, queue: deque) -> None:
+        """Admit queued requests, in queue order, while the footprint fits under the caps (one
+        request always runs)."""
+        stats = self.stats
+        while queue:
+            req = queue[0]
+            need = state_bytes(req.n, req.n)
+            if self.in_use + need > self.memory_cap and self.busy:
+                stats.cap_waits += 1
+                break
+            if (self.order == "shortest" and self.active
+                    and self.active_cells + req.n * req.n > self.cells_cap):
+                stats.cell_waits += 1
+                break
+            queue.popleft()
+            if self.active:
+                stats.joins += 1
+            sid = self.batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
+            self.in_use += need
+            self.active_cells += req.n * req.n
+            self.active[sid] = (req, self.clock())
+        stats.peak_bytes = max(stats.peak_bytes, self.in_use)
+        stats.max_active = max(stats.max_active, len(self.active))
+        stats.peak_cells = max(stats.peak_cells, self.active_cells)
+
+    def advance(self) -> list[Completion]:
+        """One round: issue the next chunk of steps, hand on the requests that had finished at
+        the previous poll while it runs, then wait for the chunk and note the newly finished.
+        Returns the completions handed on."""
+        stats, batch = self.stats, self.batch
+        if self.active:
+            batch.launch(self.chunk)  # the next chunk runs while finished requests leave
+            stats.chunks += 1
+        out = []
+        for sid, req, admitted, r, polled in self.done:
+            if self.download or self.keep_states:
+                state = batch.download(sid, out=self.results.view(_result_shape(req.n)))
+                if self.keep_states:
+                    stats.states[req.rid] = state.copy()
+            c = Completion(req.rid, req.arrival, admitted,
+                           self.clock() if self.download else polled, r.steps, r.t,
+                           req.n * req.n)
+            stats.completions.append(c)
+            out.append(c)
+            if self.on_complete is not None:
+                self.on_complete(c, stats)
+            batch.remove(sid)
+            self.in_use -= state_bytes(req.n, req.n)
+        self.done = []
+        if self.active:
+            batch.poll()
+            polled = self.clock()
+            for sid in list(self.active):
+                r, fin = batch.status(sid)
+                if fin:
+                    req, admitted = self.active.pop(sid)
+                    self.active_cells -= req.n * req.n
+                    self.done.append((sid, req, admitted, r, polled))
+        return out
+
+    def close(self) -> None:
+        self.batch.close()
+
+
 def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
           chunk: int = 16, download: bool = True, keep_states: bool = False,
           tune: bool = True, on_complete=None, order: str = "shortest",
@@ -194,79 +295,180 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
     longer wait for the long ones they would otherwise advance beside step for step. The results
     do not depend on the order (a solve's values are the same alone and in any mix).
     order="arrival" admits in arrival order under the memory cap alone."""
-    batch = BatchSolver(precision, tune=tune)
     stats = ServeStats()
-    results = ResultBuffer()
+    eng = _Engine(precision, memory_cap, chunk, download, keep_states, tune, order, cells_cap,
+                  stats, on_complete)
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     queue: deque[Request] = deque()
-    active: dict[int, tuple[Request, float]] = {}  # admitted, not finished at the last poll
-    done: list = []  # (sid, request, admitted, result, poll time) finished at the last poll
-    in_use = 0
-    active_cells = 0
-    start = time.perf_counter()
+    eng.start = time.perf_counter()
     try:
-        while pending or queue or active or done:
-            now = time.perf_counter() - start
+        while pending or queue or eng.busy:
+            now = eng.clock()
             arrived = False
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
                 arrived = True
-            if arrived and order == "shortest":
-                queue = deque(sorted(queue, key=lambda r: (r.work_estimate(), r.arrival)))
-            # admission while the footprint fits under the caps
-            while queue:
-                req = queue[0]
-                need = state_bytes(req.n, req.n)
-                if in_use + need > memory_cap and (active or done):
-                    stats.cap_waits += 1
-                    break
-                if (order == "shortest" and active
-                        and active_cells + req.n * req.n > cells_cap):
-                    stats.cell_waits += 1
-                    break
-                queue.popleft()
-                if active:
-                    stats.joins += 1
-                sid = batch.add_generated(req.n, req.n, req.init(), req.params(), req.bc)
-                in_use += need
-                active_cells += req.n * req.n
-                active[sid] = (req, time.perf_counter() - start)
-            stats.peak_bytes = max(stats.peak_bytes, in_use)
-            stats.max_active = max(stats.max_active, len(active))
-            stats.peak_cells = max(stats.peak_cells, active_cells)
-            if not active and not done:
+            if arrived:
+                queue = eng.order_queue(queue)
+            eng.admit(queue)
+            if not eng.busy:
                 if pending:
-                    time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - start)))
+                    time.sleep(max(0.0, pending[0].arrival - eng.clock()))
                 continue
-            if active:
-                batch.launch(chunk)  # the next chunk runs while finished requests leave
-                stats.chunks += 1
-            for sid, req, admitted, r, polled in done:
-                if download or keep_states:
-                    out = batch.download(sid, out=results.view(_result_shape(req.n)))
-                    if keep_states:
-                        stats.states[req.rid] = out.copy()
-                stats.completions.append(Completion(req.rid, req.arrival, admitted,
-                                                    time.perf_counter() - start if download
-                                                    else polled, r.steps, r.t, req.n * req.n))
-                if on_complete is not None:
-                    on_complete(stats.completions[-1], stats)
-                batch.remove(sid)
-                in_use -= state_bytes(req.n, req.n)
-            done = []
-            if active:
-                batch.poll()
-                polled = time.perf_counter() - start
-                for sid in list(active):
-                    r, fin = batch.status(sid)
-                    if fin:
-                        req, admitted = active.pop(sid)
-                        active_cells -= req.n * req.n
-                        done.append((sid, req, admitted, r, polled))
-        stats.makespan = time.perf_counter() - start
+            eng.advance()
+        stats.makespan = eng.clock()
     finally:
-        batch.close()
+        eng.close()
     return stats
+
+
+class Server:
+    """Online serving: requests are submitted from any thread while a worker thread runs the
+    continuous-batching engine of serve() (same admission policy, chunked advance, download of
+    finished requests while the next chunk runs).
+
+    ``submit`` returns a request id; ``poll(timeout)`` returns the completions since the last
+    poll, waiting up to ``timeout`` seconds for one; ``result(rid)`` hands over the final
+    ghosted state (9, n + 4, n + 4) of a completed request (``keep_states``); ``summary()`` gives
+    latency percentiles and throughput so far (latency counts from submission); ``close()``
+    stops taking requests, lets the submitted ones finish and stops the worker. A failed solve
+    (max_steps, a bad dt, a CUDA error) stops the worker; later calls raise its error.
+
+    ``engine_factory`` replaces the GPU engine (a callable of the ServeStats returning an object
+    with admit, advance, order_queue, busy and close; for testing the threading on a host)."""
+
+    def __init__(self, precision: int = _capi.FP32, memory_cap: float = 150e9, chunk: int = 16,
+                 order: str = "shortest", cells_cap: float = 64e6, tune: bool = True,
+                 keep_states: bool = True, engine_factory=None):
+        self.stats = ServeStats()
+        self._cond = threading.Condition()
+        self._incoming: deque[Request] = deque()
+        self._completed: list[Completion] = []
+        self._closing = False
+        self._stopped = False
+        self._error: BaseException | None = None
+        self._next_rid = 0
+        self._start = time.perf_counter()
+        if engine_factory is None:
+            def engine_factory(stats):
+                return _Engine(precision, memory_cap, chunk, True, keep_states, tune, order,
+                               cells_cap, stats, start=self._start)
+        self._factory = engine_factory
+        self._ready = threading.Event()
+        self._thread = threading.Thread(target=self._run, name="mhdb-server", daemon=True)
+        self._thread.start()
+        self._ready.wait()
+        if self._error is not None:
+            raise RuntimeError(f"server start failed: {self._error}") from self._error
+
+    def _clock(self) -> float:
+        return time.perf_counter() - self._start
+
+    def _raise_if_failed(self) -> None:
+        if self._error is not None:
+            raise RuntimeError(f"serving stopped: {self._error}") from self._error
+
+    def submit(self, n: int, t_end: float, kind: str = "fourier", seed: int = 0,
+               nonideal: bool = False, limiter: int = _capi.VANLEER,
+               gamma: float = 5.0 / 3.0) -> int:
+        """Queue a request (square grid of side n, seeded Fourier or four-quadrant state, solved
+        to t_end); returns its id."""
+        if kind not in ("fourier", "quadrants"):
+            raise ValueError(f"unknown initial state {kind!r}")
+        if int(n) < 1 or not t_end > 0.0:
+            raise ValueError("n must be positive and t_end > 0")
+        with self._cond:
+            if self._closing:
+                raise RuntimeError("server is closed")
+            self._raise_if_failed()
+            rid = self._next_rid
+            self._next_rid += 1
+            self._incoming.append(Request(rid, self._clock(), int(n), float(t_end), kind,
+                                          int(seed), bool(nonideal), float(gamma), int(limiter)))
+            self._cond.notify_all()
+        return rid
+
+    def poll(self, timeout: float = 0.0) -> list[Completion]:
+        """Completions since the last poll (waits up to timeout seconds for the first one)."""
+        with self._cond:
+            if not self._completed and timeout > 0.0:
+                self._cond.wait_for(lambda: self._completed or self._stopped, timeout)
+            out, self._completed = self._completed, []
+            if not out:
+                self._raise_if_failed()
+        return out
+
+    def result(self, rid: int) -> np.ndarray:
+        """The final state of a completed request (kept until it is taken)."""
+        with self._cond:
+            if rid not in self.stats.states:
+                raise KeyError(f"no kept result for request {rid}")
+            return self.stats.states.pop(rid)
+
+    def summary(self) -> dict:
+        with self._cond:
+            snap = ServeStats(completions=list(self.stats.completions),
+                              makespan=self._clock(), peak_bytes=self.stats.peak_bytes,
+                              max_active=self.stats.max_active, peak_cells=self.stats.peak_cells,
+                              chunks=self.stats.chunks, joins=self.stats.joins,
+                              cap_waits=self.stats.cap_waits, cell_waits=self.stats.cell_waits)
+        out = snap.summary()
+        out["submitted"] = self._next_rid
+        return out
+
+    def close(self) -> None:
+        with self._cond:
+            self._closing = True
+            self._cond.notify_all()
+        self._thread.join()
+        self._raise_if_failed()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _run(self) -> None:
+        try:
+            eng = self._factory(self.stats)
+        except BaseException as e:  # reported by the constructor
+            self._error = e
+            self._stopped = True
+            self._ready.set()
+            return
+        self._ready.set()
+        queue: deque[Request] = deque()
+        try:
+            while True:
+                with self._cond:
+                    self._cond.wait_for(lambda: self._incoming or queue or eng.busy
+                                        or self._closing)
+                    arrived = bool(self._incoming)
+                    while self._incoming:
+                        queue.append(self._incoming.popleft())
+                    if self._closing and not queue and not eng.busy:
+                        break
+                if arrived:
+                    queue = eng.order_queue(queue)
+                eng.admit(queue)
+                if not eng.busy:
+                    continue
+                done = eng.advance()
+                if done:
+                    with self._cond:
+                        self._completed.extend(done)
+                        self._cond.notify_all()
+        except BaseException as e:
+            with self._cond:
+                self._error = e
+        finally:
+            try:
+                eng.close()
+            finally:
+                with self._cond:
+                    self._stopped = True
+                    self._cond.notify_all()
 
 
 def serve_one_at_a_time(requests: list[Request], precision: int = _capi.FP64,

@@ -58,3 +58,31 @@ def test_shortest_first_admission_keeps_results_and_the_cells_cap():
         assert np.array_equal(sjf.states[req.rid], fifo.states[req.rid]), req
     steps = {c.rid: c.steps for c in fifo.completions}
     assert all(c.steps == steps[c.rid] for c in sjf.completions)
+
+
+def test_online_server_equals_serve():
+    """The online Server (worker thread, requests submitted while others run) gives every request
+    the state serve() gives it, bit for bit, with the same step count."""
+    import time
+
+    from mhd_gpu_solver_b200.serve import Server
+
+    reqs = small_stream(8, seed=13)
+    want = serve(reqs, keep_states=True)
+    steps = {c.rid: c.steps for c in want.completions}
+    with Server(keep_states=True) as srv:
+        of = {}
+        for r in reqs:
+            of[srv.submit(r.n, r.t_end, r.kind, r.seed, r.nonideal)] = r
+            time.sleep(0.002)
+        got = []
+        deadline = time.time() + 300
+        while len(got) < len(reqs) and time.time() < deadline:
+            got += srv.poll(timeout=1.0)
+        assert len(got) == len(reqs)
+        for c in got:
+            r = of[c.rid]
+            assert c.steps == steps[r.rid]
+            assert np.array_equal(srv.result(c.rid), want.states[r.rid]), r
+        s = srv.summary()
+        assert s["requests"] == len(reqs) and s["p99_ms"] >= s["p50_ms"] > 0.0

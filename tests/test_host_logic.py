@@ -210,3 +210,115 @@ def test_served_request_work_estimate():
     small = Request(rid=1, arrival=0.0, n=128, t_end=0.2, kind="quadrants", seed=1, nonideal=False)
     big = Request(rid=2, arrival=0.0, n=1024, t_end=0.2, kind="quadrants", seed=1, nonideal=False)
     assert small.work_estimate() < big.work_estimate() < ni.work_estimate() * 10
+
+
+class _FakeEngine:
+    """Stands in for the batched GPU engine: finishes each admitted request after `rounds`
+    advances (raising for request `fail_rid`), keeping a small array as its result."""
+
+    def __init__(self, stats, rounds=2, fail_rid=None):
+        import time as _t
+
+        self.stats, self.rounds, self.fail_rid = stats, rounds, fail_rid
+        self.active = {}
+        self.closed = False
+        self.t0 = _t.perf_counter()
+
+    @property
+    def busy(self):
+        return bool(self.active)
+
+    def order_queue(self, queue):
+        return queue
+
+    def admit(self, queue):
+        while queue:
+            r = queue.popleft()
+            self.active[r.rid] = [r, self.rounds]
+
+    def advance(self):
+        import time as _t
+
+        import numpy as _np
+
+        from mhd_gpu_solver_b200.serve import Completion
+
+        out = []
+        for rid, item in list(self.active.items()):
+            r, left = item
+            if rid == self.fail_rid:
+                raise RuntimeError("solve: reached max_steps before t_end")
+            if left <= 1:
+                del self.active[rid]
+                c = Completion(rid, r.arrival, r.arrival, _t.perf_counter() - self.t0, 7, r.t_end,
+                               r.n * r.n)
+                self.stats.completions.append(c)
+                self.stats.states[rid] = _np.full(3, float(rid))
+                out.append(c)
+            else:
+                item[1] = left - 1
+        return out
+
+    def close(self):
+        self.closed = True
+
+
+def test_online_server_threading_with_a_fake_engine():
+    """Server: submissions from two threads, completions through poll, results handed over once,
+    summary counts, close waits for the submitted requests and stops the worker."""
+    import threading
+
+    from mhd_gpu_solver_b200.serve import Server
+
+    engines = []
+
+    def factory(stats):
+        engines.append(_FakeEngine(stats, rounds=3))
+        return engines[-1]
+
+    srv = Server(engine_factory=factory)
+    ids = []
+
+    def submit_some(k):
+        for i in range(k):
+            ids.append(srv.submit(64 + i, 0.01, "quadrants" if i % 2 else "fourier", seed=i))
+
+    threads = [threading.Thread(target=submit_some, args=(4,)) for _ in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    got = []
+    for _ in range(200):
+        got += srv.poll(timeout=0.05)
+        if len(got) == 8:
+            break
+    assert sorted(c.rid for c in got) == sorted(ids) == list(range(8))
+    for rid in ids:
+        assert srv.result(rid)[0] == rid
+    with pytest.raises(KeyError):
+        srv.result(ids[0])  # handed over once
+    s = srv.summary()
+    assert s["requests"] == 8 and s["submitted"] == 8
+    with pytest.raises(ValueError):
+        srv.submit(64, 0.01, "vortex")
+    with pytest.raises(ValueError):
+        srv.submit(64, -1.0)
+    srv.close()
+    assert engines[0].closed
+    with pytest.raises(RuntimeError, match="closed"):
+        srv.submit(64, 0.01)
+
+
+def test_online_server_reports_a_failed_solve():
+    """A solve that fails in the worker stops it; poll and close raise the solve's error."""
+    from mhd_gpu_solver_b200.serve import Server
+
+    srv = Server(engine_factory=lambda stats: _FakeEngine(stats, rounds=2, fail_rid=1))
+    srv.submit(64, 0.01)
+    srv.submit(64, 0.01)
+    with pytest.raises(RuntimeError, match="max_steps"):
+        for _ in range(200):
+            srv.poll(timeout=0.05)
+    with pytest.raises(RuntimeError, match="max_steps"):
+        srv.close()
