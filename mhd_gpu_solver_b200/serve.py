@@ -282,7 +282,7 @@ class _Engine:
 def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: float = 150e9,
           chunk: int = 16, download: bool = True, keep_states: bool = False,
           tune: bool = True, on_complete=None, order: str = "shortest",
-          cells_cap: float = 64e6) -> ServeStats:
+          cells_cap: float = 64e6, engine_factory=None) -> ServeStats:
     """Serve a request stream in real time with continuous batching. tune: each request runs
     the batch configuration tuned for its size class (see prepare). on_complete(completion,
     stats) is called after each request finishes (progress records of long streams).
@@ -294,10 +294,14 @@ def serve(requests: list[Request], precision: int = _capi.FP32, memory_cap: floa
     64M cells keep the persistent batch kernels as busy as one 8k x 8k grid, and short requests no
     longer wait for the long ones they would otherwise advance beside step for step. The results
     do not depend on the order (a solve's values are the same alone and in any mix).
-    order="arrival" admits in arrival order under the memory cap alone."""
+    order="arrival" admits in arrival order under the memory cap alone. engine_factory(stats)
+    replaces the GPU engine (host tests, as for Server)."""
     stats = ServeStats()
-    eng = _Engine(precision, memory_cap, chunk, download, keep_states, tune, order, cells_cap,
-                  stats, on_complete)
+    if engine_factory is None:
+        eng = _Engine(precision, memory_cap, chunk, download, keep_states, tune, order,
+                      cells_cap, stats, on_complete)
+    else:
+        eng = engine_factory(stats)
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     queue: deque[Request] = deque()
     eng.start = time.perf_counter()
@@ -469,6 +473,56 @@ class Server:
                 with self._cond:
                     self._stopped = True
                     self._cond.notify_all()
+
+
+def shard_requests(requests: list[Request], world: int) -> list[list[Request]]:
+    """Split a request stream over `world` GPUs by estimated work: longest first, each onto the
+    GPU with the least estimated work so far (ties to the lower rank). Every process computes
+    the same split from the same stream; each share keeps arrival order."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    loads = [0.0] * world
+    parts: list[list[Request]] = [[] for _ in range(world)]
+    for r in sorted(requests, key=lambda r: (-r.work_estimate(), r.rid)):
+        k = min(range(world), key=lambda i: (loads[i], i))
+        parts[k].append(r)
+        loads[k] += r.work_estimate()
+    return [sorted(p, key=lambda r: (r.arrival, r.rid)) for p in parts]
+
+
+def serve_sharded(requests: list[Request], group=None, **kw) -> ServeStats:
+    """Serving sharded by request over the processes of a torch.distributed group, one GPU
+    each: every process serves its share of the stream (shard_requests) with serve(kw), with no
+    collective on the data path. The processes start together (a barrier) and afterwards
+    exchange their statistics once (all_gather_object), so every process returns the combined
+    statistics: all completions, the slowest process's makespan, the per-GPU peaks at their
+    maximum and the counters summed; kept states stay with the process that computed them.
+    Without an initialized process group this is serve()."""
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return serve(requests, **kw)
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    mine = shard_requests(requests, world)[rank]
+    dist.barrier(group=group)
+    local = serve(mine, **kw) if mine else ServeStats()
+    parts = [None] * world
+    dist.all_gather_object(parts, (local.completions, local.makespan, local.peak_bytes,
+                                   local.max_active, local.peak_cells, local.chunks, local.joins,
+                                   local.cap_waits, local.cell_waits), group=group)
+    out = ServeStats(states=local.states)
+    for comps, makespan, peak, active, cells, chunks, joins, cap, cell in parts:
+        out.completions += comps
+        out.makespan = max(out.makespan, makespan)
+        out.peak_bytes = max(out.peak_bytes, peak)
+        out.max_active = max(out.max_active, active)
+        out.peak_cells = max(out.peak_cells, cells)
+        out.chunks += chunks
+        out.joins += joins
+        out.cap_waits += cap
+        out.cell_waits += cell
+    out.completions.sort(key=lambda c: c.rid)
+    return out
 
 
 def serve_one_at_a_time(requests: list[Request], precision: int = _capi.FP64,

@@ -212,68 +212,18 @@ def test_served_request_work_estimate():
     assert small.work_estimate() < big.work_estimate() < ni.work_estimate() * 10
 
 
-class _FakeEngine:
-    """Stands in for the batched GPU engine: finishes each admitted request after `rounds`
-    advances (raising for request `fail_rid`), keeping a small array as its result."""
-
-    def __init__(self, stats, rounds=2, fail_rid=None):
-        import time as _t
-
-        self.stats, self.rounds, self.fail_rid = stats, rounds, fail_rid
-        self.active = {}
-        self.closed = False
-        self.t0 = _t.perf_counter()
-
-    @property
-    def busy(self):
-        return bool(self.active)
-
-    def order_queue(self, queue):
-        return queue
-
-    def admit(self, queue):
-        while queue:
-            r = queue.popleft()
-            self.active[r.rid] = [r, self.rounds]
-
-    def advance(self):
-        import time as _t
-
-        import numpy as _np
-
-        from mhd_gpu_solver_b200.serve import Completion
-
-        out = []
-        for rid, item in list(self.active.items()):
-            r, left = item
-            if rid == self.fail_rid:
-                raise RuntimeError("solve: reached max_steps before t_end")
-            if left <= 1:
-                del self.active[rid]
-                c = Completion(rid, r.arrival, r.arrival, _t.perf_counter() - self.t0, 7, r.t_end,
-                               r.n * r.n)
-                self.stats.completions.append(c)
-                self.stats.states[rid] = _np.full(3, float(rid))
-                out.append(c)
-            else:
-                item[1] = left - 1
-        return out
-
-    def close(self):
-        self.closed = True
-
-
 def test_online_server_threading_with_a_fake_engine():
     """Server: submissions from two threads, completions through poll, results handed over once,
     summary counts, close waits for the submitted requests and stops the worker."""
     import threading
 
     from mhd_gpu_solver_b200.serve import Server
+    from tests.serve_fakes import FakeEngine
 
     engines = []
 
     def factory(stats):
-        engines.append(_FakeEngine(stats, rounds=3))
+        engines.append(FakeEngine(stats, rounds=3))
         return engines[-1]
 
     srv = Server(engine_factory=factory)
@@ -313,8 +263,9 @@ def test_online_server_threading_with_a_fake_engine():
 def test_online_server_reports_a_failed_solve():
     """A solve that fails in the worker stops it; poll and close raise the solve's error."""
     from mhd_gpu_solver_b200.serve import Server
+    from tests.serve_fakes import FakeEngine
 
-    srv = Server(engine_factory=lambda stats: _FakeEngine(stats, rounds=2, fail_rid=1))
+    srv = Server(engine_factory=lambda stats: FakeEngine(stats, rounds=2, fail_rid=1))
     srv.submit(64, 0.01)
     srv.submit(64, 0.01)
     with pytest.raises(RuntimeError, match="max_steps"):
