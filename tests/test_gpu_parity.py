@@ -231,8 +231,9 @@ def test_resident_continuation_equals_round_trip():
     assert_components(outs[0], ref, FP64_L1)
 
 
+@pytest.mark.parametrize("config", [13, 17])
 @pytest.mark.parametrize("masked", [False, True])
-def test_increment_form_state_buffers_alternate_correctly(masked):
+def test_increment_form_state_buffers_alternate_correctly(masked, config):
     """The increment form writes U^{n+1} to the other state buffer: solves of odd and even step
     counts in sequence (7, then 40 through a captured 32-step batch and 8 direct steps, then 3)
     equal a download/upload round trip between them and, without a mask, one 50-step solve (with
@@ -246,7 +247,7 @@ def test_increment_form_state_buffers_alternate_correctly(masked):
     outs, diags = [], []
     for plan in ((7, 40, 3), (7, 40, 3, "rt"), (50,)):
         dev = _capi.DeviceSolver(nx, ny, precision=_capi.FP32)
-        dev.set_tile_config(13)
+        dev.set_tile_config(config)
         dev.configure(bc[0], bc[1], mask, True)
         dev.upload(U0)
         for n in plan:
@@ -269,7 +270,8 @@ def test_increment_form_state_buffers_alternate_correctly(masked):
     assert_components(outs[0], ref, MIXED_L1)
 
 
-def test_increment_form_time_based_solves():
+@pytest.mark.parametrize("config", [13, 17])
+def test_increment_form_time_based_solves(config):
     """Time-based solves (batches of steps between polls, graph batches and odd remainders) on
     the increment form, twice in a row on resident state: the oracle's step counts and clock,
     values within the FP32-mixed tolerance."""
@@ -279,7 +281,7 @@ def test_increment_form_time_based_solves():
     dev = _capi.DeviceSolver(nx, ny, precision=_capi.FP32)
     ref = U0
     try:
-        dev.set_tile_config(13)
+        dev.set_tile_config(config)
         dev.configure(bc[0], bc[1])
         dev.upload(U0)
         for t_end in (0.021, 0.0137):
