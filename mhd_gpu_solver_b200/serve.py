@@ -188,10 +188,11 @@ class _Engine:
 
     def __init__(self, precision: int, memory_cap: float, chunk: int, download: bool,
                  keep_states: bool, tune: bool, order: str, cells_cap: float, stats: ServeStats,
-                 on_complete=None, start: float | None = None):
+                 on_complete=None, start: float | None = None, batch=None):
         if order not in ("shortest", "arrival"):
             raise ValueError(f"unknown admission order {order!r}")
-        self.batch = BatchSolver(precision, tune=tune)
+        # batch: the BatchSolver to drive (default: a new one; host tests pass a stand-in)
+        self.batch = BatchSolver(precision, tune=tune) if batch is None else batch
         self.results = ResultBuffer()
         self.memory_cap, self.chunk, self.download = memory_cap, chunk, download
         self.keep_states, self.order, self.cells_cap = keep_states, order, cells_cap

@@ -51,3 +51,48 @@ class FakeEngine:
 
     def close(self):
         self.closed = True
+
+
+class FakeBatch:
+    """Stands in for BatchSolver under the real serving engine: solve `sid` finishes after
+    `rounds` launches; results are zero arrays of the request's ghosted shape."""
+
+    def __init__(self, rounds=2):
+        self.rounds = rounds
+        self.left = {}
+        self.shape = {}
+        self.launched = 0
+        self.removed = []
+        self.next_sid = 0
+
+    def add_generated(self, nx, ny, init, params, bc):
+        sid = self.next_sid
+        self.next_sid += 1
+        self.left[sid] = self.rounds
+        self.shape[sid] = (9, ny + 4, nx + 4)
+        return sid
+
+    def launch(self, nsteps):
+        self.launched += 1
+        for sid in self.left:
+            self.left[sid] -= 1
+
+    def poll(self):
+        return sum(1 for v in self.left.values() if v > 0)
+
+    def status(self, sid):
+        class R:
+            steps, t = 5, 0.01
+        return R(), self.left[sid] <= 0
+
+    def download(self, sid, out=None):
+        out = np.zeros(self.shape[sid]) if out is None else out
+        out[...] = 0.0
+        return out
+
+    def remove(self, sid):
+        self.removed.append(sid)
+        del self.left[sid]
+
+    def close(self):
+        pass

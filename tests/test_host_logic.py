@@ -273,3 +273,50 @@ def test_online_server_reports_a_failed_solve():
             srv.poll(timeout=0.05)
     with pytest.raises(RuntimeError, match="max_steps"):
         srv.close()
+
+
+def test_serving_engine_admission_policy_on_a_host():
+    """The serving engine's admission (serve._Engine with a stand-in batch): shortest estimated
+    work first, the cells cap (one request always runs), the memory cap in arrival order, joins
+    while others run, every request completed and removed once."""
+    from collections import deque
+
+    from mhd_gpu_solver_b200 import _capi
+    from mhd_gpu_solver_b200.serve import Request, ServeStats, _Engine, state_bytes
+    from tests.serve_fakes import FakeBatch
+
+    def stream():
+        return [Request(rid=i, arrival=0.0, n=n, t_end=0.1, kind="fourier", seed=i,
+                        nonideal=False) for i, n in enumerate([512, 128, 1024, 256])]
+
+    def run(eng, q):
+        while q or eng.busy:
+            eng.admit(q)
+            if eng.busy:
+                eng.advance()
+
+    stats, fb = ServeStats(), FakeBatch(rounds=2)
+    cap = 2 * 512 * 512
+    eng = _Engine(_capi.FP32, 150e9, 16, True, False, False, "shortest", cap, stats, batch=fb)
+    q = eng.order_queue(deque(stream()))
+    assert [r.n for r in q] == [128, 256, 512, 1024]
+    eng.admit(q)
+    assert [r.n for r in q] == [1024] and len(eng.active) == 3
+    assert stats.cell_waits == 1 and stats.joins == 2
+    run(eng, q)
+    assert sorted(c.rid for c in stats.completions) == [0, 1, 2, 3]
+    assert sorted(fb.removed) == [0, 1, 2, 3] and eng.in_use == 0 and eng.active_cells == 0
+    assert stats.peak_cells == 1024 * 1024  # the 1024^2 request ran alone, above the cap
+
+    stats, fb = ServeStats(), FakeBatch(rounds=3)
+    mem = state_bytes(1024, 1024) + state_bytes(128, 128)
+    eng = _Engine(_capi.FP32, mem, 16, True, False, False, "arrival", cap, stats, batch=fb)
+    q = eng.order_queue(deque(stream()))
+    assert [r.n for r in q] == [512, 128, 1024, 256]
+    eng.admit(q)
+    assert [r.n for r in q] == [1024, 256] and stats.cap_waits == 1
+    run(eng, q)
+    assert sorted(c.rid for c in stats.completions) == [0, 1, 2, 3]
+    assert stats.peak_bytes <= mem
+    with pytest.raises(ValueError):
+        _Engine(_capi.FP32, mem, 16, True, False, False, "fifo", cap, ServeStats(), batch=fb)
